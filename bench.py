@@ -1,0 +1,375 @@
+#!/usr/bin/env python3
+"""Benchmark of the exact APSP evaluator: evaluations per second.
+
+Default workload (N=1): one seeded random simple 16-regular graph with
+N = 65536 vertices (int32 adjacency [65536][16], 4 MiB), all 65536 sources,
+g = 1.  A step is one complete exact evaluation (diameter, integer distance
+total, ASPL) of that graph.
+
+* ``value``  -- evals/s with the adjacency already in HBM: the persistent
+  kernel timed with CUDA events on its launching stream, the L2 flushed
+  (a 512 MiB write) before every step, outside the events.
+* ``e2e``    -- the same metric through the public C ABI with host buffers
+  (ggb_eval_general: pinned staging, H2D of the adjacency, kernel, D2H of the
+  result block, synchronise), wall-clock per call.
+* ``roofline`` -- algorithmic bytes of the kernel (per executed window-level:
+  N*d*4 adjacency + N*d*W/8 gathered rows + N*W/8 own row read + N*W/8 write)
+  over its event-timed duration, against the measured HBM copy bandwidth.
+* ``cpu_baseline`` -- the reference's own OpenMP evaluator (compiled from its
+  sources into oracle/_ref) on this host's cores, over a bounded sample.
+
+``--impl reference`` times that reference CPU evaluator alone (all host
+threads) on the same workload and prints its own line.
+
+Multi-GPU (torchrun, one process per GPU): every rank evaluates its own
+seeded graph of the same size (independent objects, no collective in the data
+path), timing is bracketed by barriers and the max over ranks is taken:
+weak scaling.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "exact APSP evals/s (N=65536, d=16, all sources)"
+UNIT = "evals/s"
+WORKLOADS = {
+    "n65536d16": dict(nodes=65536, degree=16, groups=1, seed=1),
+    "n65536d16g16": dict(nodes=65536, degree=16, groups=16, seed=1),
+    "n16384d12": dict(nodes=16384, degree=12, groups=1, seed=2),
+    "n1024d8": dict(nodes=1024, degree=8, groups=1, seed=1),
+}
+
+
+def _env_int(name, default):
+    v = os.environ.get(name)
+    return int(v) if v not in (None, "") else default
+
+
+def _peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def _graph(wl: dict, rank: int):
+    from graphgolf_b200 import graphs
+    seed = wl["seed"] + 1000 * rank
+    if wl["groups"] > 1:
+        return graphs.symmetric_regular(wl["nodes"], wl["degree"], wl["groups"], seed)
+    return graphs.random_regular(wl["nodes"], wl["degree"], seed)
+
+
+class Clocks:
+    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except (OSError, ValueError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.f.flush()
+        rows = [l.split(",") for l in Path(self.f.name).read_text().splitlines() if l.strip()]
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [x.strip() for x in r]
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+            except (ValueError, IndexError):
+                continue
+            for k, name in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def algorithmic_bytes(nodes: int, degree: int, levels: int, window_bits: int) -> int:
+    """Bytes one evaluation must move, summed over its executed window-levels."""
+    row = window_bits // 8
+    return levels * (nodes * degree * 4 + nodes * degree * row + 2 * nodes * row)
+
+
+def cpu_baseline(adj, budget_s: float = 12.0):
+    """The reference OpenMP evaluator on this host, bounded to ~budget_s."""
+    import oracle
+    if not oracle.have_ref():
+        return None
+    threads = os.cpu_count() or 1
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    n = adj.shape[0]
+    # calibrate on a 1/64 share of the source chunks (the reference's MPI split)
+    t0 = time.perf_counter()
+    oracle.ref_general(adj, procs=64, rank=0)
+    t_share = time.perf_counter() - t0
+    est_full = t_share * 64
+    if est_full <= budget_s:
+        k, t0 = 0, time.perf_counter()
+        while True:
+            oracle.ref_general(adj)
+            k += 1
+            if time.perf_counter() - t0 >= budget_s or k >= 50:
+                break
+        el = time.perf_counter() - t0
+        return {"value": k / el, "unit": UNIT, "cores": threads, "kind": "reference",
+                "sample": f"{k} full evaluation(s) of the bench graph in {el:.2f} s"}
+    procs = 64
+    while procs > 1 and t_share * 64 / procs * 2 <= budget_s:
+        procs //= 2
+    t0 = time.perf_counter()
+    oracle.ref_general(adj, procs=procs, rank=0)
+    el = time.perf_counter() - t0
+    return {"value": (1.0 / procs) / el, "unit": UNIT, "cores": threads, "kind": "reference",
+            "sample": f"rank 0 of {procs} (1/{procs} of the source chunks) in {el:.2f} s"}
+
+
+def run_reference_arm(args, wl):
+    import numpy as np  # noqa: F401
+    import oracle
+    rank = _env_int("RANK", 0)
+    if rank != 0:
+        return 0
+    if not oracle.have_ref():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built from the reference "
+                          "sources (reference tree absent at build time)"}))
+        return 0
+    g = _graph(wl, 0)
+    threads = os.cpu_count() or 1
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    t0 = time.perf_counter()
+    oracle.ref_general(g.adj, procs=64, rank=0, groups=wl["groups"])
+    est_full = (time.perf_counter() - t0) * 64
+    # each step is one full evaluation unless that would take the whole run past ~3 minutes
+    procs = 1
+    while procs < 64 and est_full / procs * (args.steps + args.warmup) > 150:
+        procs *= 2
+    for _ in range(args.warmup):
+        oracle.ref_general(g.adj, procs=procs, rank=0, groups=wl["groups"])
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        oracle.ref_general(g.adj, procs=procs, rank=0, groups=wl["groups"])
+    el = time.perf_counter() - t0
+    value = args.steps / procs / el
+    sample = "one full evaluation per step" if procs == 1 else f"rank 0 of {procs} source-chunk shares per step"
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic (seeded random regular graph)",
+            "config": {"workload": args.workload, **wl}, "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def main() -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="n65536d16", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-ref-gpu", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    wl = WORKLOADS[args.workload]
+    if args.impl == "reference":
+        return run_reference_arm(args, wl)
+
+    import numpy as np
+    import torch
+
+    import graphgolf_b200 as gg
+    from graphgolf_b200 import _native
+
+    rank = _env_int("RANK", 0)
+    world = _env_int("WORLD_SIZE", 1)
+    local = _env_int("LOCAL_RANK", 0)
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    lib = gg.load()
+    if lib.ggb_init(local, wl["nodes"], wl["degree"]) != 0:
+        raise RuntimeError(_native.last_error())
+
+    g = _graph(wl, rank)
+    n, d, groups = wl["nodes"], wl["degree"], wl["groups"]
+    bn = n // groups
+    adj_dev = torch.from_numpy(np.ascontiguousarray(g.adj)).cuda()
+    stream = torch.cuda.Stream()
+    sptr = C.c_void_p(stream.cuda_stream)
+    flush = torch.empty(512 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+    res = _native.ggb_result()
+
+    def one(timed_events=None):
+        with torch.cuda.stream(stream):
+            flush.fill_(1)
+            if timed_events:
+                timed_events[0].record(stream)
+            rc = lib.ggb_launch_general_device(n, bn, groups, d, adj_dev.data_ptr(), 0, sptr)
+            if rc:
+                raise RuntimeError(_native.last_error())
+            if timed_events:
+                timed_events[1].record(stream)
+        if lib.ggb_collect(sptr, C.byref(res)):
+            raise RuntimeError(_native.last_error())
+        return res
+
+    for _ in range(args.warmup):
+        one()
+    first = gg.Result.from_c(res)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    launches0 = lib.ggb_kernel_launches()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with Clocks(local) as clk:
+        for k in range(args.steps):
+            one(evs[k])
+            assert res.total == first.total and res.diameter == first.diameter
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    launches = lib.ggb_kernel_launches() - launches0
+    per = [a.elapsed_time(b) for a, b in evs]
+    t_dev = sum(per) / 1e3
+    t_max = t_dev
+    if dist:
+        tt = torch.tensor([t_dev], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_max = float(tt.item())
+    value = world * args.steps / t_max
+    mean_ms = t_dev / args.steps * 1e3
+
+    # e2e: the public C ABI with host buffers, H2D + kernel + D2H per call
+    host_adj = np.ascontiguousarray(g.adj)
+    for _ in range(2):
+        gg.evaluate(host_adj, groups=groups)
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        r = gg.evaluate(host_adj, groups=groups)
+        assert r.total == first.total
+    e2e_t = time.perf_counter() - t0
+    e2e_max = e2e_t
+    if dist:
+        tt = torch.tensor([e2e_t], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_max = float(tt.item())
+    e2e_value = world * args.steps / e2e_max
+
+    peak, peak_kind = _peaks()
+    alg = algorithmic_bytes(n, d, first.levels, first.window_bits)
+    achieved = alg / (mean_ms / 1e3) / 1e9
+    traffic = None
+    tp = ROOT / "profiles" / f"apsp_{args.workload}_dram.json"
+    if tp.exists():
+        traffic = json.loads(tp.read_text()).get("dram_bytes_per_launch")
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": mean_ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u64",
+            "data": "synthetic (seeded random regular graph, per-pair-retry pairing model)",
+            "config": {"workload": args.workload, "nodes": n, "degree": d, "groups": groups,
+                       "sources": bn, "window_bits": first.window_bits, "windows": first.windows,
+                       "levels": first.levels, "diameter": first.diameter, "total": first.total,
+                       "l2_policy": "512 MiB flush write before every timed step (outside the events)",
+                       "parallelism": f"independent graph per rank x{world}"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured"
+                         else "fallback 6650 GB/s",
+                         "algorithmic_bytes_per_launch": alg},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": n * d * 4,
+                    "d2h_bytes_per_step": 96},
+            "gpu_launches": int(launches),
+            "clocks": clk.summary()}
+
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(host_adj)
+    if rank == 0 and world == 1 and not args.no_ref_gpu and groups == 1:
+        line["reference_cuda"] = reference_cuda(host_adj, first)
+    if rank == 0:
+        print(json.dumps(line))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def reference_cuda(adj, want):
+    """The reference's own CUDA evaluator (general/evaluation.cu, compiled for
+    sm_100a into oracle/_ref) on the same GPU: the GPU bar to beat."""
+    import oracle
+    so = oracle.REF_DIR / "libref_general_cuda.so"
+    if not so.exists():
+        return None
+    lib = C.CDLL(str(so))
+    lib.evaluation.restype = C.c_bool
+    lib.evaluation.argtypes = [C.c_int] * 5 + [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_double), C.c_int,
+                                               C.c_int]
+    lib.init_matrix_dev.argtypes = [C.c_int] * 4
+    lib.ref_set_ranks(0, 1)
+    n, d = adj.shape
+    lib.init_matrix_dev(n, d, n, 1)
+    dm, asp = C.c_int(0), C.c_double(0)
+    lib.evaluation(n, n, 1, n * d // 2, d, adj.ctypes.data, C.byref(dm), C.byref(asp), 0, 1)
+    k, t0 = 0, time.perf_counter()
+    while k < 3 or time.perf_counter() - t0 < 3.0:
+        lib.evaluation(n, n, 1, n * d // 2, d, adj.ctypes.data, C.byref(dm), C.byref(asp), 0, 1)
+        k += 1
+        if k >= 20:
+            break
+    el = time.perf_counter() - t0
+    lib.finalize_matrix_dev()
+    return {"value": k / el, "unit": UNIT, "evals": k, "same_answer": (dm.value == want.diameter
+                                                                    and asp.value == want.aspl),
+            "what": "reference general/evaluation.cu built for sm_100a, host-buffer call, wall clock"}
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,491 @@
+// apsp_core.cu -- host side of the core library libgraphgolf_b200.so.
+//
+// Owns the device state the reference keeps in module globals
+// (A_dev/B_dev/result/adjacency_dev, general/evaluation.cu:2-4): one stream,
+// grow-only device buffers, pinned staging for the adjacency and the result.
+// Every entry point is extern "C" with plain pointers (include/graphgolf_b200.h).
+//
+// Per evaluation the device does all the work of the reference's host loop
+// (general/evaluation.cu:85-112): there is no per-level launch and no
+// per-level device-to-host copy; the persistent kernel decides termination
+// itself and the host reads one 64-byte control block at the end.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cfloat>
+#include <climits>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+
+#include "../../include/graphgolf_b200.h"
+#include "apsp_kernel.cuh"
+
+namespace {
+
+using ggb::ApspArgs;
+using ggb::ApspCtrl;
+
+struct State {
+  bool ready = false;
+  int device = -1;
+  int sms = 0;
+  size_t l2_bytes = 0;
+  cudaStream_t stream = nullptr;
+  // device buffers (grow-only)
+  int* d_adj = nullptr;       size_t cap_adj = 0;     // ints
+  int* d_adj2 = nullptr;      size_t cap_adj2 = 0;    // ints (grid relabel)
+  int* d_rh = nullptr;        size_t cap_rh = 0;      // ints
+  int* d_inv = nullptr;       size_t cap_inv = 0;     // ints
+  uint4* d_bufs = nullptr;    size_t cap_buf = 0;     // uint4, both bitset matrices
+  ApspCtrl* d_ctrl = nullptr;
+  // pinned host staging
+  int* h_adj = nullptr;       size_t cap_hadj = 0;
+  int* h_rh = nullptr;        size_t cap_hrh = 0;
+  ApspCtrl* h_ctrl = nullptr;
+  // tuning
+  int force_R = 0;
+  int force_ctas = 0;
+  long long timeout_ns = 2000000000LL;
+  int phantom = 0;
+  int occ[8] = {0, 0, 0, 0, 0, 0, 0, 0};   // co-resident CTAs per SM, per R index
+  // last launch bookkeeping (for ggb_collect)
+  int last_N = 0, last_R = 0;
+  bool pending = false;
+  bool last_grid = false;
+};
+
+State g;
+std::mutex g_mu;
+char g_err[512] = "";
+long long g_launches = 0;
+
+int fail(int code, const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof g_err, fmt, ap);
+  va_end(ap);
+  return code;
+}
+
+#define CUDA_TRY(call)                                                                        \
+  do {                                                                                        \
+    cudaError_t e_ = (call);                                                                  \
+    if (e_ != cudaSuccess)                                                                    \
+      return fail(GGB_ECUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, \
+                  __LINE__);                                                                  \
+  } while (0)
+
+int r_index(int R) {
+  switch (R) {
+    case 1: return 0; case 2: return 1; case 4: return 2; case 8: return 3;
+    case 16: return 4; case 32: return 5; case 64: return 6; default: return -1;
+  }
+}
+
+const void* kernel_for(int R) {
+  switch (R) {
+    case 1: return (const void*)ggb::apsp_persistent_kernel<1>;
+    case 2: return (const void*)ggb::apsp_persistent_kernel<2>;
+    case 4: return (const void*)ggb::apsp_persistent_kernel<4>;
+    case 8: return (const void*)ggb::apsp_persistent_kernel<8>;
+    case 16: return (const void*)ggb::apsp_persistent_kernel<16>;
+    case 32: return (const void*)ggb::apsp_persistent_kernel<32>;
+    case 64: return (const void*)ggb::apsp_persistent_kernel<64>;
+    default: return nullptr;
+  }
+}
+
+int ensure_ready(int device) {
+  if (g.ready) return GGB_OK;
+  if (device < 0) {
+    int cur = 0;
+    CUDA_TRY(cudaGetDevice(&cur));
+    device = cur;
+  }
+  CUDA_TRY(cudaSetDevice(device));
+  g.device = device;
+  CUDA_TRY(cudaDeviceGetAttribute(&g.sms, cudaDevAttrMultiProcessorCount, device));
+  int l2 = 0;
+  CUDA_TRY(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, device));
+  g.l2_bytes = (size_t)l2;
+  int coop = 0;
+  CUDA_TRY(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device));
+  if (!coop) return fail(GGB_ECUDA, "device %d does not support cooperative launch", device);
+  CUDA_TRY(cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking));
+  CUDA_TRY(cudaMalloc(&g.d_ctrl, sizeof(ApspCtrl)));
+  CUDA_TRY(cudaHostAlloc(&g.h_ctrl, sizeof(ApspCtrl), cudaHostAllocDefault));
+  for (int R = 1; R <= 64; R *= 2) {
+    int nb = 0;
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel_for(R), ggb::kThreads, 0));
+    if (nb < 1) return fail(GGB_ECUDA, "persistent kernel R=%d cannot be resident", R);
+    g.occ[r_index(R)] = nb;
+  }
+  if (const char* s = getenv("GGB_BARRIER_TIMEOUT_NS")) g.timeout_ns = atoll(s);
+  g.ready = true;
+  return GGB_OK;
+}
+
+template <typename T>
+int grow_device(T** p, size_t* cap, size_t n) {
+  if (n <= *cap && *p) return GGB_OK;
+  if (*p) cudaFree(*p);
+  *p = nullptr;
+  *cap = 0;
+  size_t want = std::max<size_t>(n, 1);
+  if (cudaMalloc(p, want * sizeof(T)) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(GGB_ENOMEM, "cudaMalloc of %zu bytes failed", want * sizeof(T));
+  }
+  *cap = want;
+  return GGB_OK;
+}
+
+template <typename T>
+int grow_pinned(T** p, size_t* cap, size_t n) {
+  if (n <= *cap && *p) return GGB_OK;
+  if (*p) cudaFreeHost(*p);
+  *p = nullptr;
+  *cap = 0;
+  size_t want = std::max<size_t>(n, 1);
+  if (cudaHostAlloc(p, want * sizeof(T), cudaHostAllocDefault) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(GGB_ENOMEM, "cudaHostAlloc of %zu bytes failed", want * sizeof(T));
+  }
+  *cap = want;
+  return GGB_OK;
+}
+
+int max_ctas(int R) { return g.occ[r_index(R)] * g.sms; }
+
+// Window width: the number of uint4 per bitset row.  Both matrices of a
+// window must stay in L2 next to the adjacency, so 2*N*16*R is capped at half
+// the L2.  Among the widths that fit, the one with the least modelled time
+// wins: bytes gathered per level (d rows of 16R bytes + the d indices) over
+// all windows, plus a fixed cost per window-level for the grid barrier.
+int choose_R(int N, int d, int nsrc_max) {
+  if (g.force_R) return g.force_R;
+  const double budget = std::max<double>(8.0 * 1024 * 1024, (double)g.l2_bytes * 0.5);
+  double best = 1e300;
+  int bestR = 1;
+  for (int R = 1; R <= 64; R *= 2) {
+    const double bytes_per_buf = (double)N * 16.0 * R;
+    if (R > 1 && 2.0 * bytes_per_buf > budget) break;
+    const int W = 128 * R;
+    const long long nwin = (nsrc_max + W - 1) / W;
+    const double level_bytes = (double)N * std::max(d, 1) * (16.0 * R + 4.0) + 3.0 * bytes_per_buf;
+    const double t = nwin * (level_bytes / 8.0e12 + 3.0e-6);
+    if (t < best * 0.999) { best = t; bestR = R; }
+    if (nwin == 1) break;   // wider windows only add zero bits
+  }
+  return bestR;
+}
+
+int launch_apsp(const int* d_adj, int N, int d, int n_src1, int split, int ac, int groups,
+                int rank, int procs, cudaStream_t st) {
+  const int R = choose_R(N, d, std::max(n_src1, ac));
+  const int ri = r_index(R);
+  if (ri < 0) return fail(GGB_EINVAL, "window of %d uint4 per row is not supported", R);
+  const size_t cells = (size_t)N * R;
+  // Both matrices live in one allocation: buf0 = [0, cells), buf1 = [cells, 2*cells).
+  int rc = grow_device(&g.d_bufs, &g.cap_buf, 2 * cells);
+  if (rc) return rc;
+  const int lpr = R >= 32 ? 32 : R;
+  const int vpw = 32 / lpr;
+  long long want = ((long long)N + (long long)vpw * ggb::kWarps - 1) / ((long long)vpw * ggb::kWarps);
+  int ctas = (int)std::min<long long>(std::max<long long>(want, 1), max_ctas(R));
+  if (g.force_ctas > 0) ctas = std::min(g.force_ctas, max_ctas(R));
+
+  ApspArgs a;
+  a.adj = d_adj;
+  a.buf0 = g.d_bufs;
+  a.buf1 = g.d_bufs + cells;
+  a.ctrl = g.d_ctrl;
+  a.timeout_ns = g.timeout_ns;
+  a.N = N;
+  a.d = d;
+  a.n_src1 = n_src1;
+  a.split = split;
+  a.ac = ac;
+  a.groups = groups;
+  a.win_first = rank;
+  a.win_stride = procs;
+  a.phantom = g.phantom;
+  CUDA_TRY(cudaMemsetAsync(g.d_ctrl, 0, sizeof(ApspCtrl), st));
+  void* params[] = {(void*)&a};
+  CUDA_TRY(cudaLaunchCooperativeKernel(kernel_for(R), dim3(ctas), dim3(ggb::kThreads), params, 0, st));
+  ++g_launches;
+  g.last_N = N;
+  g.last_R = R;
+  g.pending = true;
+  return GGB_OK;
+}
+
+int read_ctrl(cudaStream_t st, ggb_partial* p) {
+  CUDA_TRY(cudaMemcpyAsync(g.h_ctrl, g.d_ctrl, sizeof(ApspCtrl), cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  g.pending = false;
+  const ApspCtrl& c = *g.h_ctrl;
+  if (c.error == ggb::kErrAdj)
+    return fail(GGB_EADJ, "adjacency entry outside [0, nodes) (reported by CTA/vertex %d)", c.error_info);
+  if (c.error == ggb::kErrPerm)
+    return fail(GGB_EPERM, "rotate_hash is not a permutation of [0, nodes) (at %d)", c.error_info);
+  if (c.error == ggb::kErrTimeout)
+    return fail(GGB_ETIMEOUT, "a grid-barrier wait ran out (CTA %d)", c.error_info);
+  if (c.error != 0) return fail(GGB_ECUDA, "device error code %d", c.error);
+  if (!c.done) return fail(GGB_ECUDA, "the persistent kernel did not complete");
+  p->diam = c.diam;
+  p->disconnected = c.disconnected;
+  p->sum = c.sum;
+  p->levels = c.levels;
+  p->windows = c.windows;
+  p->window_bits = 128 * g.last_R;
+  return GGB_OK;
+}
+
+cudaStream_t pick_stream(void* s) { return s ? (cudaStream_t)s : g.stream; }
+
+int check_general(int nodes, int based_nodes, int groups, int degree, int added_centers) {
+  if (nodes <= 0 || based_nodes <= 0 || groups <= 0 || degree < 0 || added_centers < 0)
+    return fail(GGB_EINVAL, "nodes, based_nodes, groups must be > 0 and degree, added_centers >= 0");
+  if ((long long)based_nodes * groups + added_centers != nodes)
+    return fail(GGB_EINVAL, "nodes (%d) != based_nodes*groups + added_centers (%d*%d+%d)", nodes,
+                based_nodes, groups, added_centers);
+  if ((long long)nodes * degree > INT_MAX)
+    return fail(GGB_EINVAL, "nodes*degree exceeds the int32 adjacency of the reference");
+  return GGB_OK;
+}
+
+int stage_adj(const int* adj, size_t n, cudaStream_t st) {
+  int rc = grow_device(&g.d_adj, &g.cap_adj, n);
+  if (rc) return rc;
+  rc = grow_pinned(&g.h_adj, &g.cap_hadj, n);
+  if (rc) return rc;
+  if (n) {
+    // The pinned copy must not be overwritten while a previous copy from it is
+    // in flight: the stream is idle here (every host entry point waits).
+    std::memcpy(g.h_adj, adj, n * sizeof(int));
+    CUDA_TRY(cudaMemcpyAsync(g.d_adj, g.h_adj, n * sizeof(int), cudaMemcpyHostToDevice, st));
+  }
+  return GGB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* ggb_version(void) { return "graphgolf_b200 0.1 (sm_100a)"; }
+const char* ggb_last_error(void) { return g_err; }
+long long ggb_kernel_launches(void) { return g_launches; }
+
+int ggb_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
+int ggb_init(int device, int nodes, int degree) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  int rc = ensure_ready(device);
+  if (rc) return rc;
+  if (nodes > 0 && degree >= 0) {
+    rc = grow_device(&g.d_adj, &g.cap_adj, (size_t)nodes * degree);
+    if (rc) return rc;
+    rc = grow_pinned(&g.h_adj, &g.cap_hadj, (size_t)nodes * degree);
+    if (rc) return rc;
+  }
+  return GGB_OK;
+}
+
+void ggb_finalize(void) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (!g.ready) return;
+  cudaSetDevice(g.device);
+  if (g.stream) cudaStreamSynchronize(g.stream);
+  cudaFree(g.d_adj);
+  cudaFree(g.d_adj2);
+  cudaFree(g.d_rh);
+  cudaFree(g.d_inv);
+  cudaFree(g.d_bufs);
+  cudaFree(g.d_ctrl);
+  cudaFreeHost(g.h_adj);
+  cudaFreeHost(g.h_rh);
+  cudaFreeHost(g.h_ctrl);
+  if (g.stream) cudaStreamDestroy(g.stream);
+  const int fr = g.force_R, fc = g.force_ctas;
+  g = State();
+  g.force_R = fr;
+  g.force_ctas = fc;
+}
+
+int ggb_set_tuning(int window_bits, int ctas) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (window_bits < 0 || ctas < 0) return fail(GGB_EINVAL, "negative tuning value");
+  if (window_bits) {
+    if (window_bits % 128 || r_index(window_bits / 128) < 0)
+      return fail(GGB_EINVAL, "window_bits must be 128 * (1,2,4,...,64)");
+  }
+  g.force_R = window_bits / 128;
+  g.force_ctas = ctas;
+  return GGB_OK;
+}
+
+// Test hook for the bounded waits: timeout (ns) of every grid-barrier wait
+// and a number of arrivals that never come.  phantom > 0 makes every wait run
+// out, which must surface as GGB_ETIMEOUT with the context still usable.
+int ggb_set_barrier_test(long long timeout_ns, int phantom) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (timeout_ns <= 0 || phantom < 0) return fail(GGB_EINVAL, "timeout must be > 0, phantom >= 0");
+  g.timeout_ns = timeout_ns;
+  g.phantom = phantom;
+  return GGB_OK;
+}
+
+int ggb_eval_general_partial(int nodes, int based_nodes, int groups, int degree, const int* adj,
+                             int added_centers, int rank, int procs, ggb_partial* out) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (!out || (!adj && nodes * degree)) return fail(GGB_EINVAL, "null pointer");
+  if (procs <= 0 || rank < 0 || rank >= procs) return fail(GGB_EINVAL, "rank %d of %d", rank, procs);
+  int rc = check_general(nodes, based_nodes, groups, degree, added_centers);
+  if (rc) return rc;
+  rc = ensure_ready(-1);
+  if (rc) return rc;
+  rc = stage_adj(adj, (size_t)nodes * degree, g.stream);
+  if (rc) return rc;
+  rc = launch_apsp(g.d_adj, nodes, degree, based_nodes, based_nodes * groups, added_centers, groups,
+                   rank, procs, g.stream);
+  if (rc) return rc;
+  return read_ctrl(g.stream, out);
+}
+
+int ggb_finish_general(int nodes, const ggb_partial* p, ggb_result* out) {
+  if (!p || !out) return fail(GGB_EINVAL, "null pointer");
+  out->levels = p->levels;
+  out->windows = p->windows;
+  out->window_bits = p->window_bits;
+  // general/evaluation.c:249-262: connected iff diam < nodes.
+  if (!p->disconnected && p->diam < nodes) {
+    out->connected = 1;
+    out->diameter = p->diam;
+    out->total = p->sum + (long long)nodes * (nodes - 1);
+    out->aspl = (double)out->total / (((double)nodes - 1) * nodes);
+  } else {
+    out->connected = 0;
+    out->diameter = INT_MAX;
+    out->aspl = DBL_MAX;
+    out->total = 0;
+  }
+  return GGB_OK;
+}
+
+int ggb_finish_grid(int nodes, const ggb_partial* p, ggb_result* out) {
+  if (!p || !out) return fail(GGB_EINVAL, "null pointer");
+  out->levels = p->levels;
+  out->windows = p->windows;
+  out->window_bits = p->window_bits;
+  // grid/evaluation.c:178-189: disconnected iff diameter > nodes; the
+  // diameter is written either way, ASPL only when connected.
+  const int diam = p->disconnected ? nodes + 1 : p->diam;
+  out->diameter = diam;
+  if (diam > nodes) {
+    out->connected = 0;
+    out->aspl = NAN;
+    out->total = 0;
+  } else {
+    out->connected = 1;
+    out->total = p->sum + (long long)nodes * (nodes - 1);
+    out->aspl = (double)out->total / (((double)nodes - 1) * nodes);
+  }
+  return GGB_OK;
+}
+
+int ggb_eval_general(int nodes, int based_nodes, int groups, int degree, const int* adj,
+                     int added_centers, ggb_result* out) {
+  ggb_partial p;
+  int rc = ggb_eval_general_partial(nodes, based_nodes, groups, degree, adj, added_centers, 0, 1, &p);
+  if (rc) return rc;
+  return ggb_finish_general(nodes, &p, out);
+}
+
+int ggb_launch_general_device(int nodes, int based_nodes, int groups, int degree, const int* adj_dev,
+                              int added_centers, void* stream) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (!adj_dev && nodes * degree) return fail(GGB_EINVAL, "null adjacency");
+  int rc = check_general(nodes, based_nodes, groups, degree, added_centers);
+  if (rc) return rc;
+  rc = ensure_ready(-1);
+  if (rc) return rc;
+  g.last_grid = false;
+  return launch_apsp(adj_dev, nodes, degree, based_nodes, based_nodes * groups, added_centers, groups, 0,
+                     1, pick_stream(stream));
+}
+
+int ggb_collect(void* stream, ggb_result* out) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (!out) return fail(GGB_EINVAL, "null pointer");
+  if (!g.ready) return fail(GGB_EINVAL, "nothing launched");
+  ggb_partial p;
+  int rc = read_ctrl(pick_stream(stream), &p);
+  if (rc) return rc;
+  return g.last_grid ? ggb_finish_grid(g.last_N, &p, out) : ggb_finish_general(g.last_N, &p, out);
+}
+
+int ggb_eval_general_device(int nodes, int based_nodes, int groups, int degree, const int* adj_dev,
+                            int added_centers, void* stream, ggb_result* out) {
+  int rc = ggb_launch_general_device(nodes, based_nodes, groups, degree, adj_dev, added_centers, stream);
+  if (rc) return rc;
+  return ggb_collect(stream, out);
+}
+
+int ggb_eval_grid(int nodes, int degree, int groups, const int* adj, int based_nodes,
+                  const int* rotate_hash, ggb_result* out) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (!out || !rotate_hash || (!adj && nodes * degree)) return fail(GGB_EINVAL, "null pointer");
+  if (nodes <= 0 || based_nodes <= 0 || groups <= 0 || degree < 0 || based_nodes > nodes)
+    return fail(GGB_EINVAL, "nodes, based_nodes, groups must be > 0, degree >= 0, based_nodes <= nodes");
+  if ((long long)nodes * degree > INT_MAX) return fail(GGB_EINVAL, "nodes*degree too large");
+  int rc = ensure_ready(-1);
+  if (rc) return rc;
+  const size_t n = (size_t)nodes * degree;
+  cudaStream_t st = g.stream;
+  rc = stage_adj(adj, n, st);
+  if (rc) return rc;
+  if ((rc = grow_device(&g.d_adj2, &g.cap_adj2, n))) return rc;
+  if ((rc = grow_device(&g.d_rh, &g.cap_rh, (size_t)nodes))) return rc;
+  if ((rc = grow_device(&g.d_inv, &g.cap_inv, (size_t)nodes))) return rc;
+  if ((rc = grow_pinned(&g.h_rh, &g.cap_hrh, (size_t)nodes))) return rc;
+  std::memcpy(g.h_rh, rotate_hash, (size_t)nodes * sizeof(int));
+  CUDA_TRY(cudaMemcpyAsync(g.d_rh, g.h_rh, (size_t)nodes * sizeof(int), cudaMemcpyHostToDevice, st));
+  CUDA_TRY(cudaMemsetAsync(g.d_ctrl, 0, sizeof(ApspCtrl), st));
+  CUDA_TRY(cudaMemsetAsync(g.d_inv, 0xff, (size_t)nodes * sizeof(int), st));
+  const int threads = 256;
+  const long long work = std::max<long long>((long long)n, nodes);
+  const int blocks = (int)std::min<long long>((work + threads - 1) / threads, (long long)g.sms * 8);
+  ggb::relabel_adjacency_kernel<<<blocks, threads, 0, st>>>(g.d_adj, g.d_rh, g.d_adj2, g.d_inv, nodes, degree,
+                                                            g.d_ctrl);
+  CUDA_TRY(cudaGetLastError());
+  ggb::check_permutation_kernel<<<std::min(blocks, g.sms * 4), threads, 0, st>>>(g.d_inv, nodes, g.d_ctrl);
+  CUDA_TRY(cudaGetLastError());
+  g_launches += 2;
+  CUDA_TRY(cudaMemcpyAsync(g.h_ctrl, g.d_ctrl, sizeof(ApspCtrl), cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  if (g.h_ctrl->error == ggb::kErrAdj)
+    return fail(GGB_EADJ, "adjacency entry outside [0, nodes) (row %d)", g.h_ctrl->error_info);
+  if (g.h_ctrl->error != 0)
+    return fail(GGB_EPERM, "rotate_hash is not a permutation of [0, nodes) (at %d)", g.h_ctrl->error_info);
+  g.last_grid = true;
+  rc = launch_apsp(g.d_adj2, nodes, degree, based_nodes, nodes, 0, groups, 0, 1, st);
+  if (rc) return rc;
+  ggb_partial p;
+  rc = read_ctrl(st, &p);
+  if (rc) return rc;
+  return ggb_finish_grid(nodes, &p, out);
+}
+
+}  // extern "C"

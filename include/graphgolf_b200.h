@@ -1,0 +1,198 @@
+/*
+ * graphgolf_b200.h -- C ABI of the B200 exact APSP evaluator.
+ *
+ * Two layers are declared here.
+ *
+ * 1. The core library  (graphgolf_b200/_lib/libgraphgolf_b200.so), prefix ggb_.
+ *    Plain pointers and sizes; no CUDA or torch types in any signature.  A
+ *    stream is passed as `void *` (a cudaStream_t, or NULL for the library's
+ *    own stream).
+ *
+ * 2. The drop-in shims that replace the reference's evaluator at link time:
+ *    libgg_general.so exports the general evaluation()/init_matrix_dev()/
+ *    finalize_matrix_dev() and libgg_grid.so exports the grid evaluation().
+ *    They carry the reference's names and signatures, so they are declared in
+ *    two guarded blocks below (the two evaluation() signatures clash and can
+ *    never be in one translation unit, exactly as in the reference).
+ *
+ * Numerical contract: the diameter and the integer distance total are
+ * bit-exact against the reference's CPU evaluator (general/evaluation.c,
+ * grid/evaluation.c), and ASPL is the same double, computed by the same
+ * expression from the same integer.
+ */
+#ifndef GRAPHGOLF_B200_H
+#define GRAPHGOLF_B200_H
+
+#include <stdbool.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes returned by every ggb_ function ---------------------- */
+#define GGB_OK 0
+#define GGB_EINVAL -1    /* argument out of the supported domain            */
+#define GGB_ECUDA -2     /* a CUDA runtime call failed                       */
+#define GGB_EADJ -3      /* an adjacency entry is outside [0, nodes)         */
+#define GGB_ETIMEOUT -4  /* a bounded device-side wait ran out               */
+#define GGB_EPERM -5     /* rotate_hash is not a permutation of [0, nodes)   */
+#define GGB_ENOMEM -6    /* device or pinned host memory could not be had    */
+
+/* Result of one evaluation.  `connected` is the reference evaluation()'s
+ * return value; `diameter` and `aspl` are what it writes through its
+ * pointers (see ggb_eval_general / ggb_eval_grid for the two conventions). */
+typedef struct ggb_result {
+  int connected;        /* 1: every pair reached; 0: disconnected              */
+  int diameter;         /* general: INT_MAX if disconnected; grid: nodes+1     */
+  double aspl;          /* general: DBL_MAX if disconnected; grid: NaN (the
+                           reference leaves its ASPL untouched in that case)  */
+  long long total;      /* exact Σ over ordered pairs of d(u,v), weighted by
+                           the symmetry groups = the reference's `sum` after
+                           `sum += nodes*(nodes-1)`; 0 if disconnected        */
+  long long levels;     /* BFS levels executed, summed over source windows   */
+  int windows;          /* source windows run                                 */
+  int window_bits;      /* sources per window (a multiple of 128)             */
+} ggb_result;
+
+/* Partial result of a rank that ran a strided share of the source windows
+ * (the reference's MPI decomposition, general/evaluation.c:166).  Combine
+ * partials with MAX on `diam` and SUM on `sum`, then ggb_finish_*(). */
+typedef struct ggb_partial {
+  int diam;             /* max over this rank's windows of levels-to-full (1 if none) */
+  int disconnected;     /* 1 if a window of this rank found an unreachable pair       */
+  long long sum;        /* Σ weighted unreached (vertex, source) pairs per level      */
+  long long levels;
+  int windows;
+  int window_bits;
+} ggb_partial;
+
+/* ---- lifecycle --------------------------------------------------------- */
+
+/* Selects the device for this thread and creates the library's stream and
+ * grow-only buffers for graphs up to `nodes` x `degree` (0, 0 = lazily).
+ * Replaces init_matrix_dev (general/evaluation.cu:178-194). */
+int ggb_init(int device, int nodes, int degree);
+
+/* Frees every device and pinned buffer.  Replaces finalize_matrix_dev
+ * (general/evaluation.cu:196-203).  Safe to call twice. */
+void ggb_finalize(void);
+
+/* Text of the last error on this process ("" if none). */
+const char *ggb_last_error(void);
+
+/* Library version string. */
+const char *ggb_version(void);
+
+/* Number of CUDA devices visible to this process (0 if none or on error). */
+int ggb_device_count(void);
+
+/* Forces the source-window width (bits, multiple of 128, 0 = automatic) and
+ * the persistent grid size (CTAs, 0 = automatic).  Used by the autotuner and
+ * by tests that sweep widths; results never depend on either. */
+int ggb_set_tuning(int window_bits, int ctas);
+
+/* Test hook for the bounded device waits: every grid-barrier wait gives up
+ * after timeout_ns, and `phantom` extra arrivals that never come are added to
+ * every barrier.  phantom=1 makes each wait run out, which must surface as
+ * GGB_ETIMEOUT with the CUDA context still usable.  (2e9, 0) restores the
+ * default. */
+int ggb_set_barrier_test(long long timeout_ns, int phantom);
+
+/* ---- host-buffer entry points (copy in, evaluate, copy out) ------------ */
+
+/* General graph: replaces evaluation() of general/evaluation.c:375-391 with
+ * algo MATRIX_OP / MATRIX_OP_MEM_SAVING (general/common.h:59-60), including
+ * added centres (-v).  adj is the caller's [nodes][degree] int32 array; it
+ * is read during the call only.  nodes must equal based_nodes*groups +
+ * added_centers (general/main.c:375-382).  Disconnected: connected=0,
+ * diameter=INT_MAX, aspl=DBL_MAX (general/evaluation.c:254-262). */
+int ggb_eval_general(int nodes, int based_nodes, int groups, int degree, const int *adj,
+                     int added_centers, ggb_result *out);
+
+/* Grid graph: replaces evaluation() of grid/evaluation.c:192-209 (matrix
+ * path).  rotate_hash is create_rotate_hash's relabel (grid/common.c:312-341)
+ * and must be a permutation.  Disconnected: connected=0, diameter=nodes+1 as
+ * the reference writes it, aspl=NaN (the reference leaves it untouched). */
+int ggb_eval_grid(int nodes, int degree, int groups, const int *adj, int based_nodes,
+                  const int *rotate_hash, ggb_result *out);
+
+/* ---- device-resident entry points (inputs already in HBM) -------------- */
+
+/* Same as ggb_eval_general with adj_dev a device pointer.  Enqueues on
+ * `stream` and waits for the result. */
+int ggb_eval_general_device(int nodes, int based_nodes, int groups, int degree, const int *adj_dev,
+                            int added_centers, void *stream, ggb_result *out);
+
+/* Enqueues one general evaluation on `stream` without waiting: the result
+ * stays on the device until ggb_collect() on the same stream.  Used to time
+ * back-to-back evaluations with events on the launching stream. */
+int ggb_launch_general_device(int nodes, int based_nodes, int groups, int degree, const int *adj_dev,
+                              int added_centers, void *stream);
+
+/* Waits for the last launch on `stream` and returns its result. */
+int ggb_collect(void *stream, ggb_result *out);
+
+/* Number of this library's kernels enqueued since load (each evaluation is
+ * one persistent kernel plus, for grids, two relabel kernels). */
+long long ggb_kernel_launches(void);
+
+/* ---- multi-rank decomposition (one GPU per rank) ------------------------ */
+
+/* Runs only the source windows t = rank, rank+procs, ... of a general graph
+ * (the reference's MPI split, general/evaluation.c:166,212) on this process's
+ * GPU and returns the partial.  Host buffer in, partial out. */
+int ggb_eval_general_partial(int nodes, int based_nodes, int groups, int degree, const int *adj,
+                             int added_centers, int rank, int procs, ggb_partial *out);
+
+/* Completes reduced partials into the general convention
+ * (general/evaluation.c:247-262). */
+int ggb_finish_general(int nodes, const ggb_partial *reduced, ggb_result *out);
+
+/* Completes reduced partials into the grid convention
+ * (grid/evaluation.c:176-189). */
+int ggb_finish_grid(int nodes, const ggb_partial *reduced, ggb_result *out);
+
+#ifdef __cplusplus
+}
+#endif
+
+/* ---- drop-in shim: general (link libgg_general.so instead of evaluation.o) */
+#ifdef GGB_DROPIN_GENERAL
+#ifdef __cplusplus
+extern "C" {
+#endif
+/* general/common.h:112-113 and general/evaluation.cu:205-207.  Any algo is
+ * evaluated by the bit-parallel path (MATRIX_OP and MATRIX_OP_MEM_SAVING give
+ * the same answer; the reference's CUDA evaluation also sends every algo other
+ * than MATRIX_OP down its matrix path).  Brackets TIMER_APSP through the
+ * host's timer_start/timer_stop when the host defines them. */
+bool evaluation(const int nodes, const int based_nodes, const int groups, const int lines,
+                const int degree, int *adj, int *diameter, double *ASPL,
+                const int added_centers, const int algo);
+/* general/main.c:3 and general/evaluation.cu:178: selects GPU rank % gpus
+ * and sizes the device buffers. */
+void init_matrix_dev(const int nodes, const int degree, const int based_nodes, const int algo);
+/* general/main.c:4 and general/evaluation.cu:196. */
+void finalize_matrix_dev(void);
+#ifdef __cplusplus
+}
+#endif
+#endif
+
+/* ---- drop-in shim: grid (link libgg_grid.so instead of evaluation.o) --- */
+#ifdef GGB_DROPIN_GRID
+#ifdef __cplusplus
+extern "C" {
+#endif
+/* grid/common.h:88-90.  enable_bfs selects the reference's queue BFS, whose
+ * distance total equals the matrix path's; both are served by the GPU path.
+ * No init hook exists in the grid program: buffers are created lazily. */
+bool evaluation(const int nodes, const int degree, const int groups, const int *adjacency,
+                const int based_nodes, const int height, const int based_height, int *diameter,
+                double *ASPL, const bool enable_bfs, const int *rotate_hash);
+#ifdef __cplusplus
+}
+#endif
+#endif
+
+#endif /* GRAPHGOLF_B200_H */

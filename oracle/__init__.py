@@ -1,0 +1,172 @@
+"""Test oracle for graphgolf_b200 (TEST INFRASTRUCTURE ONLY).
+
+Two checkers, both on the CPU:
+
+* ``port``: liboracle.so, this repository's plain-C restatement of the
+  reference evaluator (apsp_oracle.c, each function citing the reference
+  lines it follows).
+* ``ref``: the reference's own evaluator compiled from its sources into
+  _ref/ by the recipe in Makefile (present only where the reference source
+  tree was available at build time; the built files travel with the tree).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline and
+reference legs use this package, and only to check or time against; the
+product path never imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+REF_DIR = HERE / "_ref"
+REFERENCE_SRC = Path(os.environ.get("GGB_REFERENCE", "/root/reference"))
+
+_port = None
+_ref_general = None
+_ref_grid = None
+
+
+def build(with_reference: bool | None = None) -> None:
+    """Builds liboracle.so and, if the reference sources exist, _ref/."""
+    if with_reference is None:
+        with_reference = REFERENCE_SRC.exists()
+    targets = ["oracle"] + (["ref"] if with_reference else [])
+    subprocess.run(["make", "-s", "-C", str(HERE), f"REF={REFERENCE_SRC}", *targets], check=True)
+
+
+def port() -> C.CDLL:
+    global _port
+    if _port is None:
+        path = HERE / "liboracle.so"
+        if not path.exists():
+            build(with_reference=False)
+        lib = C.CDLL(str(path))
+        I, LL, P = C.c_int, C.c_longlong, C.c_void_p
+        IP, DP, LP = C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_longlong)
+        lib.oracle_general_eval.argtypes = [I, I, I, I, P, I, I, IP, DP, LP]
+        lib.oracle_general_partial.argtypes = [I, I, I, I, P, I, I, I, I, IP, LP]
+        lib.oracle_general_finish.argtypes = [I, I, LL, IP, DP]
+        lib.oracle_grid_eval.argtypes = [I, I, I, P, I, P, IP, DP, LP]
+        lib.oracle_grid_partial.argtypes = [I, I, I, P, I, P, I, I, IP, LP]
+        lib.oracle_grid_finish.argtypes = [I, I, LL, IP, DP]
+        lib.oracle_bfs_sums.argtypes = [I, I, P, P, I, IP, LP]
+        _port = lib
+    return _port
+
+
+def have_ref() -> bool:
+    return (REF_DIR / "libref_general.so").exists() and (REF_DIR / "libref_grid.so").exists()
+
+
+def _ref(kind: str) -> C.CDLL:
+    global _ref_general, _ref_grid
+    if kind == "general":
+        if _ref_general is None:
+            lib = C.CDLL(str(REF_DIR / "libref_general.so"))
+            lib.evaluation.restype = C.c_bool
+            lib.evaluation.argtypes = [C.c_int] * 5 + [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_double),
+                                                       C.c_int, C.c_int]
+            lib.ref_set_ranks(0, 1)
+            _ref_general = lib
+        return _ref_general
+    if _ref_grid is None:
+        lib = C.CDLL(str(REF_DIR / "libref_grid.so"))
+        lib.evaluation.restype = C.c_bool
+        lib.evaluation.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int,
+                                   C.POINTER(C.c_int), C.POINTER(C.c_double), C.c_bool, C.c_void_p]
+        lib.ref_set_ranks(0, 1)
+        _ref_grid = lib
+    return _ref_grid
+
+
+def _adj(adj) -> np.ndarray:
+    return np.ascontiguousarray(adj, dtype=np.int32)
+
+
+def general(adj, based_nodes=None, groups=1, added_centers=0, algo=1):
+    """Port: returns (connected, diameter, aspl, total)."""
+    a = _adj(adj)
+    n, d = a.shape
+    if based_nodes is None:
+        based_nodes = (n - added_centers) // groups
+    dm, asp, tot = C.c_int(0), C.c_double(0.0), C.c_longlong(0)
+    rc = port().oracle_general_eval(n, based_nodes, groups, d, a.ctypes.data, added_centers, algo,
+                                    C.byref(dm), C.byref(asp), C.byref(tot))
+    if rc < 0:
+        raise ValueError(f"oracle_general_eval: {rc}")
+    return bool(rc), dm.value, asp.value, tot.value
+
+
+def general_partial(adj, rank, procs, based_nodes=None, groups=1, added_centers=0):
+    """Port: rank's partial (diam, sum) before the MPI_Allreduce."""
+    a = _adj(adj)
+    n, d = a.shape
+    if based_nodes is None:
+        based_nodes = (n - added_centers) // groups
+    dm, sm = C.c_int(0), C.c_longlong(0)
+    rc = port().oracle_general_partial(n, based_nodes, groups, d, a.ctypes.data, added_centers, 0, rank, procs,
+                                       C.byref(dm), C.byref(sm))
+    if rc < 0:
+        raise ValueError(f"oracle_general_partial: {rc}")
+    return dm.value, sm.value
+
+
+def grid(adj, rotate_hash, groups=1, based_nodes=None):
+    """Port: returns (connected, diameter, aspl or None, total)."""
+    a = _adj(adj)
+    n, d = a.shape
+    rh = np.ascontiguousarray(rotate_hash, dtype=np.int32)
+    if based_nodes is None:
+        based_nodes = n // groups
+    dm, asp, tot = C.c_int(0), C.c_double(float("nan")), C.c_longlong(0)
+    rc = port().oracle_grid_eval(n, d, groups, a.ctypes.data, based_nodes, rh.ctypes.data, C.byref(dm),
+                                 C.byref(asp), C.byref(tot))
+    if rc < 0:
+        raise ValueError(f"oracle_grid_eval: {rc}")
+    return bool(rc), dm.value, (asp.value if rc else None), tot.value
+
+
+def bfs_sums(adj, n_sources=None, relabel=None):
+    """Plain queue BFS: (max eccentricity or -1, Σ distances from the sources)."""
+    a = _adj(adj)
+    n, d = a.shape
+    rh = None if relabel is None else np.ascontiguousarray(relabel, dtype=np.int32)
+    e, s = C.c_int(0), C.c_longlong(0)
+    port().oracle_bfs_sums(n, d, a.ctypes.data, None if rh is None else rh.ctypes.data,
+                           n if n_sources is None else n_sources, C.byref(e), C.byref(s))
+    return e.value, s.value
+
+
+def ref_general(adj, based_nodes=None, groups=1, added_centers=0, algo=1, procs=1, rank=0):
+    """Reference general evaluation() (compiled from its sources):
+    returns (connected, diameter, aspl)."""
+    lib = _ref("general")
+    a = _adj(adj)
+    n, d = a.shape
+    if based_nodes is None:
+        based_nodes = (n - added_centers) // groups
+    lib.ref_set_ranks(rank, procs)
+    dm, asp = C.c_int(0), C.c_double(0.0)
+    ok = lib.evaluation(n, based_nodes, groups, n * d // 2, d, a.ctypes.data, C.byref(dm), C.byref(asp),
+                        added_centers, algo)
+    lib.ref_set_ranks(0, 1)
+    return bool(ok), dm.value, asp.value
+
+
+def ref_grid(adj, rotate_hash, groups=1, based_nodes=None, height=0, based_height=0, enable_bfs=False):
+    """Reference grid evaluation(): returns (connected, diameter, aspl or None)."""
+    lib = _ref("grid")
+    a = _adj(adj)
+    n, d = a.shape
+    rh = np.ascontiguousarray(rotate_hash, dtype=np.int32)
+    if based_nodes is None:
+        based_nodes = n // groups
+    dm, asp = C.c_int(0), C.c_double(float("nan"))
+    ok = lib.evaluation(n, d, groups, a.ctypes.data, based_nodes, height, based_height, C.byref(dm),
+                        C.byref(asp), bool(enable_bfs), rh.ctypes.data)
+    return bool(ok), dm.value, (asp.value if ok else None)
