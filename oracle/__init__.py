@@ -99,7 +99,8 @@ def general(adj, based_nodes=None, groups=1, added_centers=0, algo=1):
                                     C.byref(dm), C.byref(asp), C.byref(tot))
     if rc < 0:
         raise ValueError(f"oracle_general_eval: {rc}")
-    return bool(rc), dm.value, asp.value, tot.value
+    # the reference divides nothing for a disconnected graph: no total then
+    return bool(rc), dm.value, asp.value, (tot.value if rc else 0)
 
 
 def general_partial(adj, rank, procs, based_nodes=None, groups=1, added_centers=0):
@@ -128,7 +129,7 @@ def grid(adj, rotate_hash, groups=1, based_nodes=None):
                                  C.byref(asp), C.byref(tot))
     if rc < 0:
         raise ValueError(f"oracle_grid_eval: {rc}")
-    return bool(rc), dm.value, (asp.value if rc else None), tot.value
+    return bool(rc), dm.value, (asp.value if rc else None), (tot.value if rc else 0)
 
 
 def bfs_sums(adj, n_sources=None, relabel=None):
