@@ -123,8 +123,21 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def algorithmic_bytes(nodes: int, degree: int, levels: int, window_bits: int) -> int:
-    """Bytes one evaluation must move, summed over its executed window-levels."""
+def algorithmic_bytes(nodes: int, degree: int, dense_levels: int, windows: int, window_bits: int) -> int:
+    """Bytes one evaluation must move.  Per dense sweep of a window: the
+    adjacency (N*d*4), the d gathered rows of every vertex (N*d*W/8), its own
+    row read and the new row written (2*N*W/8).  Per window, the seeding of
+    the first two levels: the two-hop adjacency (N*(d+d^2)*4) and two rows
+    written (2*N*W/8)."""
+    row = window_bits // 8
+    dense = dense_levels * (nodes * degree * 4 + nodes * degree * row + 2 * nodes * row)
+    seed = windows * (nodes * (degree + degree * degree) * 4 + 2 * nodes * row)
+    return dense + seed
+
+
+def survey_formula_bytes(nodes: int, degree: int, levels: int, window_bits: int) -> int:
+    """The same figure if every executed level were a dense sweep (the
+    reference algorithm's work at this window width)."""
     row = window_bits // 8
     return levels * (nodes * degree * 4 + nodes * degree * row + 2 * nodes * row)
 
@@ -210,6 +223,10 @@ def main() -> int:
     ap.add_argument("--workload", default="n65536d16", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ref-gpu", action="store_true")
+    ap.add_argument("--flush-mib", type=int, default=512, help="L2 flush buffer written before every step")
+    ap.add_argument("--window-bits", type=int, default=0, help="force the source-window width (0 = automatic)")
+    ap.add_argument("--ball", type=int, default=-1, choices=[-1, 0, 1],
+                    help="ball pre-pass policy: -1 automatic, 0 never, 1 whenever feasible")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     wl = WORKLOADS[args.workload]
@@ -234,6 +251,9 @@ def main() -> int:
     lib = gg.load()
     if lib.ggb_init(local, wl["nodes"], wl["degree"]) != 0:
         raise RuntimeError(_native.last_error())
+    if args.window_bits:
+        gg.set_tuning(args.window_bits, 0)
+    gg.set_ball(args.ball)
 
     g = _graph(wl, rank)
     n, d, groups = wl["nodes"], wl["degree"], wl["groups"]
@@ -241,7 +261,7 @@ def main() -> int:
     adj_dev = torch.from_numpy(np.ascontiguousarray(g.adj)).cuda()
     stream = torch.cuda.Stream()
     sptr = C.c_void_p(stream.cuda_stream)
-    flush = torch.empty(512 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+    flush = torch.empty(max(args.flush_mib, 200) * 1024 * 1024, dtype=torch.uint8, device="cuda")
     res = _native.ggb_result()
 
     def one(timed_events=None):
@@ -303,7 +323,7 @@ def main() -> int:
     e2e_value = world * args.steps / e2e_max
 
     peak, peak_kind = _peaks()
-    alg = algorithmic_bytes(n, d, first.levels, first.window_bits)
+    alg = algorithmic_bytes(n, d, first.dense_levels, first.windows, first.window_bits)
     achieved = alg / (mean_ms / 1e3) / 1e9
     traffic = None
     tp = ROOT / "profiles" / f"apsp_{args.workload}_dram.json"
@@ -316,14 +336,17 @@ def main() -> int:
             "data": "synthetic (seeded random regular graph, per-pair-retry pairing model)",
             "config": {"workload": args.workload, "nodes": n, "degree": d, "groups": groups,
                        "sources": bn, "window_bits": first.window_bits, "windows": first.windows,
-                       "levels": first.levels, "diameter": first.diameter, "total": first.total,
-                       "l2_policy": "512 MiB flush write before every timed step (outside the events)",
+                       "levels": first.levels, "dense_levels": first.dense_levels,
+                       "diameter": first.diameter, "total": first.total,
+                       "l2_policy": f"{max(args.flush_mib, 200)} MiB flush write before every timed step (outside the events)",
                        "parallelism": f"independent graph per rank x{world}"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured"
                          else "fallback 6650 GB/s",
-                         "algorithmic_bytes_per_launch": alg},
+                         "algorithmic_bytes_per_launch": alg,
+                         "survey_formula_bytes_per_launch": survey_formula_bytes(n, d, first.levels,
+                                                                                 first.window_bits)},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": n * d * 4,
                     "d2h_bytes_per_step": 96},
             "gpu_launches": int(launches),

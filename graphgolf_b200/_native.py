@@ -30,6 +30,7 @@ class ggb_result(C.Structure):
         ("levels", C.c_longlong),
         ("windows", C.c_int),
         ("window_bits", C.c_int),
+        ("dense_levels", C.c_longlong),
     ]
 
 
@@ -43,6 +44,7 @@ class ggb_partial(C.Structure):
         ("levels", C.c_longlong),
         ("windows", C.c_int),
         ("window_bits", C.c_int),
+        ("dense_levels", C.c_longlong),
     ]
 
 
@@ -58,6 +60,7 @@ CORE_SIGNATURES = {
     "ggb_version": (C.c_char_p, []),
     "ggb_device_count": (_I, []),
     "ggb_set_tuning": (_I, [_I, _I]),
+    "ggb_set_ball": (_I, [_I]),
     "ggb_set_barrier_test": (_I, [_LL, _I]),
     "ggb_eval_general": (_I, [_I, _I, _I, _I, _P, _I, C.POINTER(ggb_result)]),
     "ggb_eval_grid": (_I, [_I, _I, _I, _P, _I, _P, C.POINTER(ggb_result)]),
@@ -65,6 +68,8 @@ CORE_SIGNATURES = {
     "ggb_launch_general_device": (_I, [_I, _I, _I, _I, _P, _I, _P]),
     "ggb_collect": (_I, [_P, C.POINTER(ggb_result)]),
     "ggb_kernel_launches": (_LL, []),
+    "ggb_trace_enable": (_I, [_I]),
+    "ggb_trace_read": (_I, [_P, _I]),
     "ggb_eval_general_partial": (_I, [_I, _I, _I, _I, _P, _I, _I, _I, C.POINTER(ggb_partial)]),
     "ggb_finish_general": (_I, [_I, C.POINTER(ggb_partial), C.POINTER(ggb_result)]),
     "ggb_finish_grid": (_I, [_I, C.POINTER(ggb_partial), C.POINTER(ggb_result)]),

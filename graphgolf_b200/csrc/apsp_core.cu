@@ -19,6 +19,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <cstdint>
 #include <mutex>
 
 #include "../../include/graphgolf_b200.h"
@@ -51,7 +52,15 @@ struct State {
   int force_ctas = 0;
   long long timeout_ns = 2000000000LL;
   int phantom = 0;
+  uint4* d_ball = nullptr;    size_t cap_ball = 0;    // uint4, ball pre-pass matrix
+  unsigned long long* d_ball_cnt = nullptr; size_t cap_ball_cnt = 0;
+  int ball_mode = -1;         // -1 automatic, 0 never, 1 whenever feasible
+  int ball_occ = 0;           // co-resident ball CTAs per SM at the last size
+  long long* d_trace = nullptr;   // optional barrier trace (ggb_trace_enable)
+  int trace_cap = 0;
+  int trace_len = 0;
   int occ[8] = {0, 0, 0, 0, 0, 0, 0, 0};   // co-resident CTAs per SM, per R index
+  int smem_optin = 0;
   // last launch bookkeeping (for ggb_collect)
   int last_N = 0, last_R = 0;
   bool pending = false;
@@ -99,6 +108,19 @@ const void* kernel_for(int R) {
   }
 }
 
+size_t smem_for(int R) {
+  switch (R) {
+    case 1: return ggb::apsp_smem_bytes<1>();
+    case 2: return ggb::apsp_smem_bytes<2>();
+    case 4: return ggb::apsp_smem_bytes<4>();
+    case 8: return ggb::apsp_smem_bytes<8>();
+    case 16: return ggb::apsp_smem_bytes<16>();
+    case 32: return ggb::apsp_smem_bytes<32>();
+    case 64: return ggb::apsp_smem_bytes<64>();
+    default: return 0;
+  }
+}
+
 int ensure_ready(int device) {
   if (g.ready) return GGB_OK;
   if (device < 0) {
@@ -120,10 +142,18 @@ int ensure_ready(int device) {
   CUDA_TRY(cudaHostAlloc(&g.h_ctrl, sizeof(ApspCtrl), cudaHostAllocDefault));
   for (int R = 1; R <= 64; R *= 2) {
     int nb = 0;
-    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel_for(R), ggb::kThreads, 0));
+    CUDA_TRY(cudaFuncSetAttribute(kernel_for(R), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_for(R)));
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel_for(R), ggb::kThreads, smem_for(R)));
     if (nb < 1) return fail(GGB_ECUDA, "persistent kernel R=%d cannot be resident", R);
     g.occ[r_index(R)] = nb;
   }
+  int smem_optin = 0;
+  CUDA_TRY(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+  g.smem_optin = smem_optin;
+  CUDA_TRY(cudaFuncSetAttribute((const void*)ggb::ball_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                smem_optin - 4096));
+  CUDA_TRY(cudaFuncSetAttribute((const void*)ggb::ball_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                smem_optin - 4096));
   if (const char* s = getenv("GGB_BARRIER_TIMEOUT_NS")) g.timeout_ns = atoll(s);
   g.ready = true;
   return GGB_OK;
@@ -162,22 +192,26 @@ int grow_pinned(T** p, size_t* cap, size_t n) {
 int max_ctas(int R) { return g.occ[r_index(R)] * g.sms; }
 
 // Window width: the number of uint4 per bitset row.  Both matrices of a
-// window must stay in L2 next to the adjacency, so 2*N*16*R is capped at half
-// the L2.  Among the widths that fit, the one with the least modelled time
-// wins: bytes gathered per level (d rows of 16R bytes + the d indices) over
-// all windows, plus a fixed cost per window-level for the grid barrier.
+// window must stay in L2 next to the adjacency, so 2*N*16*R is capped at 55%
+// of the L2.  Among the widths that fit, the one with the least modelled time
+// wins: per window, the two-hop seeding (d + d^2 adjacency reads and two row
+// writes per vertex) plus about four dense sweeps of d gathered rows of 16R
+// bytes, at the L2 gather rate, plus a fixed cost per sweep for the grid
+// barrier.  Results never depend on the choice.
 int choose_R(int N, int d, int nsrc_max) {
   if (g.force_R) return g.force_R;
-  const double budget = std::max<double>(8.0 * 1024 * 1024, (double)g.l2_bytes * 0.5);
+  const double budget = std::max<double>(8.0 * 1024 * 1024, (double)g.l2_bytes * 0.55);
   double best = 1e300;
   int bestR = 1;
+  const double dd = std::max(d, 1);
   for (int R = 1; R <= 64; R *= 2) {
     const double bytes_per_buf = (double)N * 16.0 * R;
     if (R > 1 && 2.0 * bytes_per_buf > budget) break;
     const int W = 128 * R;
     const long long nwin = (nsrc_max + W - 1) / W;
-    const double level_bytes = (double)N * std::max(d, 1) * (16.0 * R + 4.0) + 3.0 * bytes_per_buf;
-    const double t = nwin * (level_bytes / 8.0e12 + 3.0e-6);
+    const double seed_bytes = (double)N * (dd + dd * dd) * 4.0 + 2.0 * bytes_per_buf;
+    const double level_bytes = (double)N * dd * (16.0 * R + 4.0) + 2.0 * bytes_per_buf;
+    const double t = nwin * ((seed_bytes + 4.0 * level_bytes) / 14.0e12 + 5.0 * 2.5e-6);
     if (t < best * 0.999) { best = t; bestR = R; }
     if (nwin == 1) break;   // wider windows only add zero bits
   }
@@ -199,6 +233,34 @@ int launch_apsp(const int* d_adj, int N, int d, int n_src1, int split, int ac, i
   int ctas = (int)std::min<long long>(std::max<long long>(want, 1), max_ctas(R));
   if (g.force_ctas > 0) ctas = std::min(g.force_ctas, max_ctas(R));
 
+  // Ball pre-pass: worth it when its one-off cost (d + d^2 + d^3 adjacency
+  // reads per vertex, one HBM write of every window's S_3 rows) is below what
+  // it saves (per window: the two-hop seeding and one dense sweep).
+  const bool vec4 = (d % 4 == 0 && ((uintptr_t)d_adj % 16) == 0);
+  const int W = 128 * R;
+  const int nwin1 = n_src1 > 0 ? (n_src1 + W - 1) / W : 0;
+  const int n_local = nwin1 > rank ? (nwin1 - rank + procs - 1) / procs : 0;
+  const size_t ball_cells = (size_t)n_local * N * R;
+  const size_t ball_smem = ggb::ball_smem_bytes(n_src1, d, std::max(n_local, 1));
+  bool use_ball = g.ball_mode != 0 && ac == 0 && n_local >= 1 && n_local <= ggb::kBallMaxWindows && d >= 1 &&
+                  d <= ggb::kBallMaxDegree && ball_smem <= (size_t)(g.smem_optin - 4096) &&
+                  ball_cells * 16 <= ((size_t)8 << 30);
+  if (use_ball && g.ball_mode < 0) {
+    const double dd = d;
+    const double t_ball = (double)N * (dd + dd * dd + dd * dd * dd) * 4.0 / 12.0e12 +
+                          (double)ball_cells * 16.0 / 6.0e12 + 10.0e-6;
+    const double level = (double)N * dd * (16.0 * R + 4.0) / 14.0e12 + 2.5e-6;
+    const double seed = (double)N * (dd + dd * dd) * 4.0 / 12.0e12 + (double)N * 16.0 * R / 8.0e12 + 2.5e-6;
+    use_ball = t_ball < 0.8 * n_local * (level + seed);
+  }
+  if (use_ball) {
+    rc = grow_device(&g.d_ball, &g.cap_ball, ball_cells);
+    if (rc) return rc;
+    rc = grow_device(&g.d_ball_cnt, &g.cap_ball_cnt, (size_t)n_local * 6);
+    if (rc) return rc;
+    CUDA_TRY(cudaMemsetAsync(g.d_ball_cnt, 0, (size_t)n_local * 6 * sizeof(unsigned long long), st));
+  }
+
   ApspArgs a;
   a.adj = d_adj;
   a.buf0 = g.d_bufs;
@@ -214,9 +276,42 @@ int launch_apsp(const int* d_adj, int N, int d, int n_src1, int split, int ac, i
   a.win_first = rank;
   a.win_stride = procs;
   a.phantom = g.phantom;
+  a.trace = g.d_trace;
+  a.trace_cap = g.trace_cap;
+  a.vec4 = vec4 ? 1 : 0;
+  a.ball = use_ball ? g.d_ball : nullptr;
+  a.ball_cnt = use_ball ? g.d_ball_cnt : nullptr;
   CUDA_TRY(cudaMemsetAsync(g.d_ctrl, 0, sizeof(ApspCtrl), st));
+  if (use_ball) {
+    ggb::BallArgs b;
+    b.adj = d_adj;
+    b.ball = g.d_ball;
+    b.cnt = g.d_ball_cnt;
+    b.ctrl = g.d_ctrl;
+    b.N = N;
+    b.d = d;
+    b.n_src = n_src1;
+    b.split = split;
+    b.R = R;
+    b.win_first = rank;
+    b.win_stride = procs;
+    b.n_local = n_local;
+    const void* bk = vec4 ? (const void*)ggb::ball_kernel<4> : (const void*)ggb::ball_kernel<1>;
+    int nb = 0;
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, bk, ggb::kBallThreads, ball_smem));
+    if (nb < 1) return fail(GGB_ECUDA, "ball pre-pass cannot be resident with %zu bytes of shared memory", ball_smem);
+    g.ball_occ = nb;
+    const long long need = ((long long)N + ggb::kBallThreads / 32 - 1) / (ggb::kBallThreads / 32);
+    const int bgrid = (int)std::min<long long>(need, (long long)nb * g.sms);
+    if (vec4)
+      ggb::ball_kernel<4><<<bgrid, ggb::kBallThreads, ball_smem, st>>>(b);
+    else
+      ggb::ball_kernel<1><<<bgrid, ggb::kBallThreads, ball_smem, st>>>(b);
+    CUDA_TRY(cudaGetLastError());
+    ++g_launches;
+  }
   void* params[] = {(void*)&a};
-  CUDA_TRY(cudaLaunchCooperativeKernel(kernel_for(R), dim3(ctas), dim3(ggb::kThreads), params, 0, st));
+  CUDA_TRY(cudaLaunchCooperativeKernel(kernel_for(R), dim3(ctas), dim3(ggb::kThreads), params, smem_for(R), st));
   ++g_launches;
   g.last_N = N;
   g.last_R = R;
@@ -241,8 +336,10 @@ int read_ctrl(cudaStream_t st, ggb_partial* p) {
   p->disconnected = c.disconnected;
   p->sum = c.sum;
   p->levels = c.levels;
+  p->dense_levels = c.dense_levels;
   p->windows = c.windows;
   p->window_bits = 128 * g.last_R;
+  g.trace_len = c.trace_len;
   return GGB_OK;
 }
 
@@ -314,14 +411,18 @@ void ggb_finalize(void) {
   cudaFree(g.d_inv);
   cudaFree(g.d_bufs);
   cudaFree(g.d_ctrl);
+  cudaFree(g.d_trace);
+  cudaFree(g.d_ball);
+  cudaFree(g.d_ball_cnt);
   cudaFreeHost(g.h_adj);
   cudaFreeHost(g.h_rh);
   cudaFreeHost(g.h_ctrl);
   if (g.stream) cudaStreamDestroy(g.stream);
-  const int fr = g.force_R, fc = g.force_ctas;
+  const int fr = g.force_R, fc = g.force_ctas, bm = g.ball_mode;
   g = State();
   g.force_R = fr;
   g.force_ctas = fc;
+  g.ball_mode = bm;
 }
 
 int ggb_set_tuning(int window_bits, int ctas) {
@@ -336,6 +437,15 @@ int ggb_set_tuning(int window_bits, int ctas) {
   return GGB_OK;
 }
 
+// Ball pre-pass policy: -1 automatic (cost model), 0 never, 1 whenever the
+// sizes allow it.  Results never depend on the choice.
+int ggb_set_ball(int mode) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (mode < -1 || mode > 1) return fail(GGB_EINVAL, "ball mode must be -1, 0 or 1");
+  g.ball_mode = mode;
+  return GGB_OK;
+}
+
 // Test hook for the bounded waits: timeout (ns) of every grid-barrier wait
 // and a number of arrivals that never come.  phantom > 0 makes every wait run
 // out, which must surface as GGB_ETIMEOUT with the context still usable.
@@ -345,6 +455,33 @@ int ggb_set_barrier_test(long long timeout_ns, int phantom) {
   g.timeout_ns = timeout_ns;
   g.phantom = phantom;
   return GGB_OK;
+}
+
+// Barrier trace: with capacity > 0, CTA 0 records (globaltimer ns, tag) after
+// every grid barrier of the following evaluations; 0 turns it off.
+int ggb_trace_enable(int capacity) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  int rc = ensure_ready(-1);
+  if (rc) return rc;
+  if (g.d_trace) cudaFree(g.d_trace);
+  g.d_trace = nullptr;
+  g.trace_cap = 0;
+  g.trace_len = 0;
+  if (capacity > 0) {
+    CUDA_TRY(cudaMalloc(&g.d_trace, (size_t)capacity * 2 * sizeof(long long)));
+    g.trace_cap = capacity;
+  }
+  return GGB_OK;
+}
+
+// Copies the trace of the last evaluation (pairs of long long) to `out`;
+// returns the number of pairs, or a negative error.
+int ggb_trace_read(long long* out, int max_pairs) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (!g.d_trace) return 0;
+  const int n = std::min(g.trace_len, max_pairs);
+  if (n > 0) CUDA_TRY(cudaMemcpy(out, g.d_trace, (size_t)n * 2 * sizeof(long long), cudaMemcpyDeviceToHost));
+  return n;
 }
 
 int ggb_eval_general_partial(int nodes, int based_nodes, int groups, int degree, const int* adj,
@@ -367,6 +504,7 @@ int ggb_eval_general_partial(int nodes, int based_nodes, int groups, int degree,
 int ggb_finish_general(int nodes, const ggb_partial* p, ggb_result* out) {
   if (!p || !out) return fail(GGB_EINVAL, "null pointer");
   out->levels = p->levels;
+  out->dense_levels = p->dense_levels;
   out->windows = p->windows;
   out->window_bits = p->window_bits;
   // general/evaluation.c:249-262: connected iff diam < nodes.
@@ -387,6 +525,7 @@ int ggb_finish_general(int nodes, const ggb_partial* p, ggb_result* out) {
 int ggb_finish_grid(int nodes, const ggb_partial* p, ggb_result* out) {
   if (!p || !out) return fail(GGB_EINVAL, "null pointer");
   out->levels = p->levels;
+  out->dense_levels = p->dense_levels;
   out->windows = p->windows;
   out->window_bits = p->window_bits;
   // grid/evaluation.c:178-189: disconnected iff diameter > nodes; the

@@ -1,24 +1,36 @@
-// apsp_kernel.cuh -- the persistent bit-parallel BFS kernel (sm_100a).
+// apsp_kernel.cuh -- the bit-parallel BFS kernels (sm_100a).
 //
-// One launch evaluates one graph.  The sources are cut into windows of
-// W = 128*R bits; a window keeps two bitset matrices S_cur and S_prev of
-// nodes x W bits, small enough to stay resident in the 126 MB L2 while the
-// window runs.  Every level is one sweep of all CTAs over all vertices:
+// One evaluation = (optionally) one ball pre-pass kernel + one persistent
+// cooperative kernel.  The sources are cut into windows of W = 128*R bits; a
+// window keeps two bitset matrices of nodes x W bits, small enough to stay
+// resident in the 126 MB L2 while the window runs.  Every dense level is one
+// sweep of all CTAs over all vertices:
 //
-//     S_next[v] = S_prev[v] | OR_{j<d} S_cur[adj[v][j]]          (*)
+//     S_{k+1}[v] = S_k[v] | OR_{j<d} S_k[adj[v][j]]                      (*)
 //
-// which is the reference's recurrence B |= A[adj]; swap(A,B)
-// (general/evaluation.c:175-181,194-197, grid/evaluation.c:143-151).  The
-// popcount of S_next is reduced in the same sweep (warp shuffles, one 64-bit
-// atomic per CTA), and after a bounded-spin grid barrier every CTA reads the
-// level's count and takes the same decision the reference takes on the host:
-// stop when all (vertex, source) pairs are reached (:192), else add the
-// unreached pairs times the group weight to the sum (:199-200).
+// The reference's recurrence is S_{k+1}[v] = S_{k-1}[v] | OR_j S_k[adj[v][j]]
+// (B |= A[adj]; swap(A,B), general/evaluation.c:175-181,194-197,
+// grid/evaluation.c:143-151).  Both give the same sets for ANY adjacency:
+// the reference's sets are monotone (S_{k-1} <= S_k, by induction from
+// S_{-1} = S_0 = identity), so S_{k-1}[v] <= S_k[v], and
+// S_k[v] = S_{k-2}[v] | OR_j S_{k-1}[u_j] <= S_{k-1}[v] | OR_j S_k[u_j].
+// Using S_k[v] makes the destination matrix write-only.
 //
-// A window also stops when a level adds no bit at all.  (*) makes every
-// per-source set monotone, and a level that adds nothing is a fixed point, so
-// the reference would run on to kk == nodes and report a disconnected graph;
-// stopping there gives the identical answer without the N-level walk.
+// The popcount of S_{k+1} is reduced in the same sweep (warp shuffles, one
+// 64-bit atomic per CTA), and after a bounded-spin grid barrier every CTA
+// reads the level's count and takes the decision the reference takes on the
+// host: stop when all (vertex, source) pairs are reached (:192), else add the
+// unreached pairs times the group weight to the sum (:199-200).  A window also
+// stops when a level adds no bit at all: the sets are monotone, a level that
+// adds nothing is a fixed point, and the reference would run on to
+// kk == nodes and report a disconnected graph -- the identical answer.
+//
+// The first levels of a window are not swept.  Either
+//  - the ball pre-pass (ball_kernel) has written S_3 of every window into a
+//    window-major matrix in HBM together with the exact counts of S_1..S_3,
+//    and dense sweeps start at S_4; or
+//  - the window's first step builds S_2 directly from the two-hop adjacency
+//    (seed_window) and dense sweeps start at S_3.
 //
 // Bitset rows are read with ld.global.cg (L2, no L1 allocation): rows written
 // by other SMs in the previous level must never be served from a stale L1
@@ -30,8 +42,11 @@
 
 namespace ggb {
 
-constexpr int kThreads = 512;         // threads per CTA
+constexpr int kThreads = 512;         // threads per CTA (one CTA per SM, up to 128 registers per thread)
 constexpr int kWarps = kThreads / 32;
+constexpr int kBallThreads = 256;     // threads per CTA of the ball pre-pass
+constexpr int kBallMaxWindows = 32;   // windows of one rank in the ball pre-pass (one per lane)
+constexpr int kBallMaxDegree = 32;
 
 // Error codes written to ApspCtrl::error (host maps them to GGB_E*).
 enum : int { kErrNone = 0, kErrAdj = 1, kErrTimeout = 2, kErrPerm = 3 };
@@ -39,7 +54,7 @@ enum : int { kErrNone = 0, kErrAdj = 1, kErrTimeout = 2, kErrPerm = 3 };
 // Device-side control block.  Zeroed by the host before every launch.
 struct ApspCtrl {
   unsigned long long bar;         // grid-barrier arrivals (monotone)
-  unsigned long long cnt[2][2];   // [level parity][lo rows, hi rows] cumulative popcounts
+  unsigned long long cnt[4][2];   // [level mod 4][lo rows, hi rows] cumulative popcounts
   int error;                      // first error code
   int error_info;                 // e.g. the offending vertex
   // outputs (written by CTA 0, thread 0, at the end)
@@ -47,7 +62,9 @@ struct ApspCtrl {
   int disconnected;
   long long sum;                  // Σ weighted unreached pairs (before + N(N-1))
   long long levels;               // levels executed over all windows
+  long long dense_levels;         // of which dense OR-gather sweeps
   int windows;
+  int trace_len;                  // trace pairs written
   int done;                       // 1 once the outputs are written
 };
 
@@ -63,6 +80,11 @@ struct ApspArgs {
   int ac;                // added centres: phase-2 sources are rows N-ac .. N-1
   int groups;
   int win_first, win_stride;   // this rank's windows: t = win_first + k*win_stride
+  int vec4;              // 1: degree % 4 == 0 and adj 16-byte aligned (vector adjacency loads)
+  const uint4* ball;     // phase-1 S_3 rows, [local window][N][R], or null (two-hop seeding)
+  const unsigned long long* ball_cnt;  // [local window][3][lo, hi]: counts of S_1 and S_2 (slot 2 unused)
+  long long* trace;      // optional: (globaltimer ns, tag) pairs written by CTA 0 after every barrier
+  int trace_cap;         // pairs available in trace
   int phantom;           // extra arrivals every barrier waits for: 0 in normal use; the
                          // fault-path test sets 1 so that every bounded wait runs out
 };
@@ -127,19 +149,501 @@ __device__ __forceinline__ unsigned popc4(const uint4& a) {
   return __popc(a.x) + __popc(a.y) + __popc(a.z) + __popc(a.w);
 }
 
+// Popcount bookkeeping of one BFS level, identical in every CTA: returns 1
+// when the window is complete (reference :192), 2 when the level added no bit
+// (a fixed point: the reference would report a disconnected graph), else adds
+// the unreached pairs to the sum (:199-200) and returns 0.
+__device__ __forceinline__ int level_decision(int phase, long long lvl_lo, long long lvl_hi, long long l,
+                                              long long N, long long lo_rows, long long hi_rows, long long groups,
+                                              long long& prev_total, long long& sum) {
+  const long long total = lvl_lo + lvl_hi;
+  const bool full = phase == 1 ? (total == N * l) : (lvl_hi == hi_rows * l);
+  if (full) return 1;
+  if (total == prev_total) return 2;
+  if (phase == 1) {
+    sum += (lo_rows * l - lvl_lo) * groups;
+    sum += (hi_rows * l - lvl_hi) * 2 * groups;
+  } else {
+    sum += hi_rows * l - lvl_hi;
+  }
+  prev_total = total;
+  return 0;
+}
+
+// Trace record after a barrier (CTA 0, thread 0 only; no-op without a buffer).
+// tag: 1 = seeding of a window done, 2 = dense sweep done; the level kk is
+// stored above the tag byte.
+__device__ __forceinline__ void trace_mark(const ApspArgs& a, int& n, int tag, long long kk) {
+  if (a.trace && blockIdx.x == 0 && threadIdx.x == 0 && n < a.trace_cap) {
+    a.trace[2 * n] = (long long)globaltimer_ns();
+    a.trace[2 * n + 1] = (kk << 8) | tag;
+    ++n;
+  }
+}
+
+// Sums NV per-thread counters over the CTA; thread 0 adds value i to
+// ctrl->cnt[(g0 + i/2) & 3][i & 1] (lo/hi counts of one or two levels).
+template <int NV>
+__device__ __forceinline__ void cta_add_counts(const unsigned* c, ApspCtrl* ctrl, unsigned g0,
+                                               unsigned long long (*s_red)[4]) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  unsigned long long r[NV];
+#pragma unroll
+  for (int i = 0; i < NV; ++i) r[i] = c[i];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+    for (int i = 0; i < NV; ++i) r[i] += __shfl_xor_sync(0xffffffffu, r[i], o);
+  if (lane == 0)
+#pragma unroll
+    for (int i = 0; i < NV; ++i) s_red[warp][i] = r[i];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int i = 0; i < NV; ++i) {
+      unsigned long long b = 0;
+      for (int w = 0; w < kWarps; ++w) b += s_red[w][i];
+      if (b) atomicAdd(&ctrl->cnt[(g0 + i / 2) & 3][i & 1], b);
+    }
+  }
+}
+
+// After the barrier that ends `nl` levels (1 or 2), thread 0 reads their
+// cumulative counts, turns them into per-level counts with the values it saw
+// last time, and publishes them in s_lvl[0..2*nl).  Every CTA reads the same
+// counter values (no CTA can add to these slots again before all CTAs have
+// passed the next barrier), so all take identical decisions.
+__device__ __forceinline__ void read_level_counts(ApspCtrl* ctrl, unsigned g0, int nl,
+                                                  unsigned long long (*s_seen)[2], long long* s_lvl) {
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < nl; ++i) {
+      const unsigned slot = (g0 + i) & 3;
+      const unsigned long long lo = ld_acquire_u64(&ctrl->cnt[slot][0]);
+      const unsigned long long hi = ld_acquire_u64(&ctrl->cnt[slot][1]);
+      s_lvl[2 * i] = (long long)(lo - s_seen[slot][0]);
+      s_lvl[2 * i + 1] = (long long)(hi - s_seen[slot][1]);
+      s_seen[slot][0] = lo;
+      s_seen[slot][1] = hi;
+    }
+  }
+  __syncthreads();
+}
+
+// ---- adjacency loads ---------------------------------------------------------
+template <int VEC> struct AdjVec;
+template <> struct AdjVec<1> {
+  int v;
+  __device__ __forceinline__ void load(const int* p) { v = __ldg(p); }
+  __device__ __forceinline__ int at(int) const { return v; }
+};
+template <> struct AdjVec<4> {
+  int4 v;
+  __device__ __forceinline__ void load(const int* p) { v = __ldg(reinterpret_cast<const int4*>(p)); }
+  __device__ __forceinline__ int at(int i) const { return i == 0 ? v.x : i == 1 ? v.y : i == 2 ? v.z : v.w; }
+};
+
+// OR `v` into a 32-bit word of shared memory with a shared-space reduction
+// (the pointer is turned into a shared-window address, so the compiler can
+// never fall back to a generic atomic).
+__device__ __forceinline__ void smem_or(unsigned* p, unsigned v) {
+  const unsigned addr = (unsigned)__cvta_generic_to_shared(p);
+  asm volatile("red.shared.or.b32 [%0], %1;" ::"r"(addr), "r"(v) : "memory");
+}
+
+// OR `v` into a shared word and return the previous value.
+__device__ __forceinline__ unsigned smem_or_old(unsigned* p, unsigned v) {
+  const unsigned addr = (unsigned)__cvta_generic_to_shared(p);
+  unsigned old;
+  asm volatile("atom.shared.or.b32 %0, [%1], %2;" : "=r"(old) : "r"(addr), "r"(v) : "memory");
+  return old;
+}
+
+__device__ __forceinline__ void set_bit_in(unsigned* row, int x, int base, int nbits) {
+  const unsigned b = (unsigned)(x - base);
+  if (b < (unsigned)nbits) smem_or(row + (b >> 5), 1u << (b & 31));
+}
+
+// Sets, in `row`, bit (x - base) of every entry x of the `nrows` adjacency
+// rows whose ids are ids[0..nrows) when 0 <= x - base < nbits (row ids are
+// checked against N; an entry outside [0, N) clears adj_ok).  The G lanes of
+// a group split each row into its d/VEC vectors: when a row has at most G
+// vectors, lane r always loads vector r % per of rows r / per, r / per + G/per,
+// ... so a lane's loads follow a fixed pattern with no division in the loop;
+// longer rows are taken one at a time.  Up to 8 loads are in flight per lane
+// and the bit sets are predicated, not branched.  With out_ids, entry e of
+// row j is also stored at out_ids[j*d + e] (-1 for an invalid row id).
+// Per-lane count of newly set bits by window, in shared memory: lane L owns
+// the column col = base + L of a [window][32] array, so counting never
+// conflicts or needs an atomic.  Bit b lies in global window b >> log2w; only
+// this rank's windows (first, first + stride, ...) are counted.
+struct NewBitCount {
+  unsigned* col;
+  int log2w, first, stride, nwin;
+  __device__ __forceinline__ void add(unsigned b) const {
+    int k = (int)(b >> log2w) - first;
+    if (k < 0) return;
+    if (stride != 1) {
+      if (k % stride) return;
+      k /= stride;
+    }
+    if (k < nwin) col[k * 32] += 1u;
+  }
+};
+
+__device__ __forceinline__ void set_bit_counted(unsigned* row, unsigned b, const NewBitCount* nbc) {
+  const unsigned m = 1u << (b & 31);
+  if (nbc) {
+    if (!(smem_or_old(row + (b >> 5), m) & m)) nbc->add(b);
+  } else {
+    smem_or(row + (b >> 5), m);
+  }
+}
+
+template <int VEC, int G>
+__device__ __forceinline__ void set_rows_bits(const int* __restrict__ adj, int N, int d, const int* ids, int nrows,
+                                              unsigned* row, int base, int nbits, int r, bool& adj_ok,
+                                              int* out_ids, const NewBitCount* nbc = nullptr) {
+  const int per = d / VEC;
+  bool bad = false;
+  if (per <= G) {
+    const int rpi = G / per;                 // rows per group step
+    const bool active = r < rpi * per;
+    const int roff = r / per, part = r - roff * per;
+    for (int r0 = 0; r0 < nrows; r0 += rpi * 8) {
+      AdjVec<VEC> val[8];
+      bool ok[8];
+      int pos[8];
+#pragma unroll
+      for (int t = 0; t < 8; ++t) {
+        const int j = r0 + t * rpi + roff;
+        const bool in = active && j < nrows;
+        const int u = in ? ids[j] : -1;
+        ok[t] = in && (unsigned)u < (unsigned)N;
+        pos[t] = in ? j * d + part * VEC : -1;
+        if (ok[t]) val[t].load(adj + (long long)u * d + part * VEC);
+      }
+#pragma unroll
+      for (int t = 0; t < 8; ++t) {
+#pragma unroll
+        for (int e = 0; e < VEC; ++e) {
+          const int x = ok[t] ? val[t].at(e) : -1;
+          if (out_ids && pos[t] >= 0) out_ids[pos[t] + e] = x;
+          bad |= ok[t] && (unsigned)x >= (unsigned)N;
+          const unsigned b = (unsigned)(x - base);
+          if (ok[t] && b < (unsigned)nbits) set_bit_counted(row, b, nbc);
+        }
+      }
+    }
+  } else {
+    for (int j = 0; j < nrows; ++j) {
+      const int u = ids[j];
+      const bool okr = (unsigned)u < (unsigned)N;
+      for (int p0 = 0; p0 < per; p0 += G * 8) {
+        AdjVec<VEC> val[8];
+        bool ok[8];
+#pragma unroll
+        for (int t = 0; t < 8; ++t) {
+          const int part = p0 + t * G + r;
+          ok[t] = okr && part < per;
+          if (ok[t]) val[t].load(adj + (long long)u * d + part * VEC);
+          if (out_ids && !okr && part < per)
+#pragma unroll
+            for (int e = 0; e < VEC; ++e) out_ids[j * d + part * VEC + e] = -1;
+        }
+#pragma unroll
+        for (int t = 0; t < 8; ++t) {
+          const int part = p0 + t * G + r;
+#pragma unroll
+          for (int e = 0; e < VEC; ++e) {
+            const int x = ok[t] ? val[t].at(e) : -1;
+            if (out_ids && ok[t]) out_ids[j * d + part * VEC + e] = x;
+            bad |= ok[t] && (unsigned)x >= (unsigned)N;
+            const unsigned b = (unsigned)(x - base);
+            if (ok[t] && b < (unsigned)nbits) set_bit_counted(row, b, nbc);
+          }
+        }
+      }
+    }
+  }
+  if (bad) adj_ok = false;
+}
+
+// ---- per-window seeding: S_2 from the two-hop adjacency ----------------------
+constexpr int kSeedGroup = 8;                    // lanes per vertex
+constexpr int kSeedVerts = 32 / kSeedGroup;      // vertices per warp and step
+constexpr int kSeedNb = 64;                      // neighbour ids staged per vertex and pass
+
+// Builds S_1 (counted only) and S_2 (-> s2_out) rows of every vertex for the
+// window whose bit 0 is vertex `base`, counting their bits into c[4] (S_1
+// lo/hi, S_2 lo/hi):  S_1[v] = {v} u adj[v][*] and
+// S_2[v] = S_1[v] u U_j adj[u_j][*] restricted to the window, which is (*)
+// applied twice to the identity.  A warp takes 4 vertices per step, 8 lanes
+// each: the lanes stage the vertex's neighbour ids in shared memory, set the
+// bits of v and its neighbours, then load the neighbours' adjacency rows and
+// set the bits of every two-hop vertex; the warp then writes the 4 S_2 rows
+// out coalesced.  Replaces the reference's clear + identity set-up (:168-172)
+// and its first two OR-gather sweeps.
+template <int R, int VEC>
+__device__ __forceinline__ void seed_window(const ApspArgs& a, int base, int l, uint4* s2_out, int* s_nb,
+                                            unsigned* s_rw, unsigned (&c)[4], bool& adj_ok, long long warp_id,
+                                            long long n_warps) {
+  constexpr int SROW = 4 * R;
+  const int N = a.N, d = a.d;
+  const int lane = threadIdx.x & 31, g = lane / kSeedGroup, r = lane % kSeedGroup;
+  uint4* const rows4 = reinterpret_cast<uint4*>(s_rw);
+  int* const nb = s_nb + g * kSeedNb;
+  unsigned* const s1 = s_rw + (2 * g) * SROW;
+  unsigned* const s2 = s1 + SROW;
+  for (long long v0 = warp_id * kSeedVerts; v0 < N; v0 += n_warps * kSeedVerts) {
+    for (int i = lane; i < 2 * kSeedVerts * R; i += 32) rows4[i] = make_uint4(0u, 0u, 0u, 0u);
+    const long long v = v0 + g;
+    const bool live = v < N;
+    __syncwarp();   // rows zeroed before any bit is set
+    if (live && r == 0) set_bit_in(s1, (int)v, base, l);
+    for (int jb = 0; jb < d; jb += kSeedNb) {
+      const int dc = min(kSeedNb, d - jb);
+      __syncwarp();
+      if (live)
+        for (int j = r; j < dc; j += kSeedGroup) nb[j] = __ldg(a.adj + v * d + jb + j);
+      __syncwarp();
+      if (!live) continue;
+      for (int j = r; j < dc; j += kSeedGroup) {
+        const int x = nb[j];
+        if ((unsigned)x >= (unsigned)N) { adj_ok = false; continue; }
+        set_bit_in(s1, x, base, l);
+      }
+      set_rows_bits<VEC, kSeedGroup>(a.adj, N, d, nb, dc, s2, base, l, r, adj_ok, nullptr);
+    }
+    __syncwarp();
+#pragma unroll
+    for (int i = 0; i < kSeedVerts; ++i) {
+      const long long vi = v0 + i;
+      if (vi >= N) break;
+      unsigned c1 = 0, c2 = 0;
+      for (int col = lane; col < R; col += 32) {
+        const uint4 x1 = rows4[(2 * i) * R + col];
+        uint4 x2 = rows4[(2 * i + 1) * R + col];
+        or_into(x2, x1);   // S_2 includes S_1
+        st_cg(s2_out + vi * R + col, x2);
+        c1 += popc4(x1);
+        c2 += popc4(x2);
+      }
+      if (vi < a.split) { c[0] += c1; c[2] += c2; } else { c[1] += c1; c[3] += c2; }
+    }
+    __syncwarp();
+  }
+}
+
+// ---- the ball pre-pass: S_3 of every window at once --------------------------
+//
+// One warp per vertex v builds, in shared memory, the row of all phase-1
+// sources within three applications of (*) from v:
+//     S_1[v] = {v} u N(v),  S_2[v] = S_1[v] u N(N(v)),  S_3[v] = S_2[v] u N(N(N(v)))
+// (N(x) = adj[x][*]; exact for any adjacency), counting after each step the
+// bits that fall into every window of this rank, and finally writes the S_3
+// segment of every window to ball[local window][v].  That is 1 + d + d^2 + d^3
+// adjacency entries per vertex read once per evaluation, instead of the two
+// seeding steps and the first dense sweep of every window.
+struct BallArgs {
+  const int* adj;
+  uint4* ball;                    // [local windows][N][R]
+  unsigned long long* cnt;        // [local windows][3][2], zeroed by the host
+  ApspCtrl* ctrl;                 // error reporting
+  int N, d, n_src, split;
+  int R;                          // uint4 per window row
+  int win_first, win_stride, n_local;
+};
+
+// uint4 of one full ball row (all phase-1 sources), padded to a multiple of 4.
+__host__ __device__ __forceinline__ int ball_row_u4(int n_src) { return ((n_src + 127) / 128 + 3) / 4 * 4; }
+
+// Shared memory of one warp of ball_kernel, in uint4: the full row, the one-
+// and two-hop neighbour ids (d + d^2 ints, padded) and the per-lane new-bit
+// counters of S_1 and S_2 for nwin windows.
+__host__ __device__ __forceinline__ int ball_warp_u4(int n_src, int d, int nwin) {
+  return ball_row_u4(n_src) + (d + d * d + 3) / 4 + 2 * nwin * 32 / 4;
+}
+
+// The ball pre-pass runs only without added centres (every row is a "lo"
+// row) and with at most 32 windows per rank.  It writes the counts of S_1
+// and S_2 per window (counted exactly, as new bits, while they are set); the
+// count of S_3 is taken by the window's first dense sweep, which reads every
+// S_3 row anyway.
+template <int VEC>
+__global__ void __launch_bounds__(kBallThreads, 2) ball_kernel(const BallArgs b) {
+  extern __shared__ uint4 s_ball[];
+  constexpr int kWarpsB = kBallThreads / 32;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int N = b.N, d = b.d, R = b.R;
+  const int nwin = b.n_local;
+  const int row_u4 = ball_row_u4(b.n_src);
+  uint4* const row4 = s_ball + (size_t)warp * ball_warp_u4(b.n_src, d, nwin);
+  unsigned* const row = reinterpret_cast<unsigned*>(row4);
+  int* const nb1 = reinterpret_cast<int*>(row4 + row_u4);
+  int* const nb2 = nb1 + d;
+  unsigned* const lc = reinterpret_cast<unsigned*>(row4 + row_u4 + (d + d * d + 3) / 4);  // [2][nwin][32]
+  for (int i = lane; i < 2 * nwin * 32; i += 32) lc[i] = 0u;
+  int log2w = 0;
+  while ((128 * R) >> log2w > 1) ++log2w;
+  const NewBitCount c1{lc + lane, log2w, b.win_first, b.win_stride, nwin};
+  const NewBitCount c2{lc + nwin * 32 + lane, log2w, b.win_first, b.win_stride, nwin};
+  bool adj_ok = true;
+  const long long warp_id = (long long)blockIdx.x * kWarpsB + warp;
+  const long long n_warps = (long long)gridDim.x * kWarpsB;
+  for (long long v = warp_id; v < N; v += n_warps) {
+    for (int i = lane; i < row_u4; i += 32) row4[i] = make_uint4(0u, 0u, 0u, 0u);
+    for (int j = lane; j < d; j += 32) nb1[j] = __ldg(b.adj + v * d + j);
+    __syncwarp();
+    // S_1 = {v} u N(v)
+    if (lane == 0 && v < b.n_src) set_bit_counted(row, (unsigned)v, &c1);
+    for (int j = lane; j < d; j += 32) {
+      const int x = nb1[j];
+      if ((unsigned)x >= (unsigned)N) { adj_ok = false; continue; }
+      if (x < b.n_src) set_bit_counted(row, (unsigned)x, &c1);
+    }
+    __syncwarp();
+    // S_2 = S_1 u N(N(v))
+    set_rows_bits<VEC, 32>(b.adj, N, d, nb1, d, row, 0, b.n_src, lane, adj_ok, nb2, &c2);
+    __syncwarp();
+    // S_3 = S_2 u N(N(N(v)))
+    set_rows_bits<VEC, 32>(b.adj, N, d, nb2, d * d, row, 0, b.n_src, lane, adj_ok, nullptr, nullptr);
+    __syncwarp();
+    for (int k = 0; k < nwin; ++k) {
+      const int t = b.win_first + k * b.win_stride;
+      uint4* dst = b.ball + ((size_t)k * N + v) * R;
+      for (int col = lane; col < R; col += 32) {
+        const int idx = t * R + col;
+        st_cg(dst + col, idx < row_u4 ? row4[idx] : make_uint4(0u, 0u, 0u, 0u));
+      }
+    }
+    __syncwarp();
+  }
+  if (!adj_ok) set_error(b.ctrl, kErrAdj, (int)blockIdx.x);
+  // lane k sums window k's columns: S_1 = new bits of step 1, S_2 = S_1 + new bits of step 2
+  if (lane < nwin) {
+    unsigned long long s1 = 0, s2 = 0;
+    for (int i = 0; i < 32; ++i) {
+      s1 += lc[lane * 32 + i];
+      s2 += lc[nwin * 32 + lane * 32 + i];
+    }
+    if (s1) atomicAdd(b.cnt + (size_t)lane * 6 + 0, s1);
+    if (s1 + s2) atomicAdd(b.cnt + (size_t)lane * 6 + 2, s1 + s2);
+  }
+}
+
+// Shared memory of ball_kernel, in bytes.
+inline size_t ball_smem_bytes(int n_src, int d, int nwin) {
+  return (size_t)(kBallThreads / 32) * (size_t)ball_warp_u4(n_src, d, nwin) * sizeof(uint4);
+}
+
+// ---- one dense sweep, wide rows ------------------------------------------------
+// Valid-bit mask of the 128-bit chunk `col` of a row of a window with l sources.
+__device__ __forceinline__ uint4 chunk_full_mask(int col, int l) {
+  const int nvalid = max(0, min(128, l - 128 * col));
+  unsigned m[4];
+#pragma unroll
+  for (int w = 0; w < 4; ++w) {
+    const int vw = max(0, min(32, nvalid - 32 * w));
+    m[w] = vw == 32 ? 0xffffffffu : ((1u << vw) - 1u);
+  }
+  return make_uint4(m[0], m[1], m[2], m[3]);
+}
+
+__device__ __forceinline__ bool equal4(const uint4& a, const uint4& b) {
+  return a.x == b.x && a.y == b.y && a.z == b.z && a.w == b.w;
+}
+
+// One sweep of (*) for rows of R >= 32 uint4 (one warp per row, lane L owns
+// uint4 L, L+32, ...) and degree d <= 32.  Lane j holds the neighbour id u_j
+// of the current vertex and hands it to the warp by shuffle; the next
+// vertex's ids and own row are loaded while the current gathers are in
+// flight, so a vertex costs one memory round trip.  A lane whose chunk of the
+// vertex's own row is already full (every valid bit set) loads nothing: the OR
+// cannot change it.  Near the last level, when most rows are almost full,
+// this drops most of the gathered sectors.
+template <int R>
+__device__ __forceinline__ void sweep_wide(const uint4* __restrict__ src, uint4* __restrict__ dst,
+                                           const int* __restrict__ adj, int N, int d, int split, long long v0,
+                                           long long stride, int l, bool own_count, unsigned (&cl)[4],
+                                           bool& adj_ok) {
+  constexpr int UPL = R / 32;
+  constexpr int U = UPL >= 2 ? 8 : 16;
+  const int lane = threadIdx.x & 31;
+  uint4 fm[UPL];
+#pragma unroll
+  for (int k = 0; k < UPL; ++k) fm[k] = chunk_full_mask(lane + 32 * k, l);
+  int u_nx = 0;
+  uint4 own_nx[UPL];
+#pragma unroll
+  for (int k = 0; k < UPL; ++k) own_nx[k] = make_uint4(0u, 0u, 0u, 0u);
+  if (v0 < N) {
+    u_nx = lane < d ? __ldg(adj + v0 * d + lane) : 0;
+#pragma unroll
+    for (int k = 0; k < UPL; ++k) own_nx[k] = ld_cg(src + v0 * R + lane + 32 * k);
+  }
+  for (long long v = v0; v < N; v += stride) {
+    int u_me = u_nx;
+    uint4 acc[UPL];
+#pragma unroll
+    for (int k = 0; k < UPL; ++k) acc[k] = own_nx[k];
+    const long long vn = v + stride;
+    if (vn < N) {
+      u_nx = lane < d ? __ldg(adj + vn * d + lane) : 0;
+#pragma unroll
+      for (int k = 0; k < UPL; ++k) own_nx[k] = ld_cg(src + vn * R + lane + 32 * k);
+    }
+    if (lane < d && (unsigned)u_me >= (unsigned)N) { adj_ok = false; u_me = 0; }
+    if (own_count) {
+      unsigned co = 0;
+#pragma unroll
+      for (int k = 0; k < UPL; ++k) co += popc4(acc[k]);
+      if (v < split) cl[2] += co; else cl[3] += co;
+    }
+    bool need[UPL];
+#pragma unroll
+    for (int k = 0; k < UPL; ++k) need[k] = !equal4(acc[k], fm[k]);
+    for (int j0 = 0; j0 < d; j0 += U) {
+      uint4 x[U][UPL];
+#pragma unroll
+      for (int q = 0; q < U; ++q) {
+        const int j = j0 + q;
+        const int u = __shfl_sync(0xffffffffu, u_me, j & 31);
+#pragma unroll
+        for (int k = 0; k < UPL; ++k)
+          x[q][k] = (j < d && need[k]) ? ld_cg(src + (long long)u * R + lane + 32 * k) : make_uint4(0u, 0u, 0u, 0u);
+      }
+#pragma unroll
+      for (int q = 0; q < U; ++q)
+#pragma unroll
+        for (int k = 0; k < UPL; ++k) or_into(acc[k], x[q][k]);
+    }
+    unsigned cc = 0;
+#pragma unroll
+    for (int k = 0; k < UPL; ++k) {
+      st_cg(dst + v * R + lane + 32 * k, acc[k]);
+      cc += popc4(acc[k]);
+    }
+    if (v < split) cl[0] += cc; else cl[1] += cc;
+  }
+}
+
+// ---- the persistent kernel -----------------------------------------------------
 // R = uint4 words per row (W = 128*R source bits).  LPR lanes share a row,
 // each lane owning UPL uint4 of it; a warp covers VPW vertices per step.
 template <int R>
-__global__ void __launch_bounds__(kThreads, 2) apsp_persistent_kernel(const ApspArgs a) {
+__global__ void __launch_bounds__(kThreads, 1) apsp_persistent_kernel(const ApspArgs a) {
   constexpr int LPR = R >= 32 ? 32 : R;
   constexpr int VPW = 32 / LPR;
   constexpr int UPL = R / LPR;
   constexpr int W = 128 * R;
-  constexpr int U = UPL >= 2 ? 2 : 8;  // neighbour rows in flight per thread
+  constexpr int U = UPL >= 2 ? 8 : 16;  // neighbour rows in flight per thread
+  constexpr int SROW = 4 * R;          // 32-bit words per row in shared memory
 
-  __shared__ unsigned long long s_red[kWarps][2];
-  __shared__ unsigned long long s_cnt[2];
+  __shared__ unsigned long long s_red[kWarps][4];
+  __shared__ unsigned long long s_seen[4][2];
+  __shared__ long long s_lvl[4];
   __shared__ int s_flag;
+  extern __shared__ unsigned s_dyn[];   // per warp: neighbour ids [4][64], then rows [4][2][SROW]
 
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
@@ -149,11 +653,23 @@ __global__ void __launch_bounds__(kThreads, 2) apsp_persistent_kernel(const Apsp
   const long long n_slots = (long long)gridDim.x * kWarps * VPW;
   const int N = a.N, d = a.d;
   const unsigned grid = gridDim.x;
+  int* const my_nb = reinterpret_cast<int*>(s_dyn) + (size_t)warp * (kSeedVerts * kSeedNb + 2 * kSeedVerts * SROW);
+  unsigned* const my_rows = reinterpret_cast<unsigned*>(my_nb + kSeedVerts * kSeedNb);
+  const long long warp_id = (long long)blockIdx.x * kWarps + warp;
+  const long long n_warps = (long long)gridDim.x * kWarps;
 
   unsigned long long bar_target = 0;
-  unsigned long long seen[2][2] = {{0ULL, 0ULL}, {0ULL, 0ULL}};
-  unsigned gl = 0;                     // global level counter (parity selects cnt slot)
-  long long sum = 0, levels = 0;
+  // Level counts live in cnt[gl & 3]: between two barriers a CTA adds to the
+  // slots of at most two levels while slower CTAs may still read the (at most
+  // two) slots of the levels that ended at the previous barrier; four slots
+  // keep those sets disjoint.  The counters only grow; s_seen holds the value
+  // this CTA read last time, so a level's count is the difference.
+  if (threadIdx.x < 8) s_seen[threadIdx.x >> 1][threadIdx.x & 1] = 0ULL;
+  __syncthreads();
+  unsigned gl = 0;                     // global level counter
+  int ntrace = 0;
+  trace_mark(a, ntrace, 0, 0);
+  long long sum = 0, levels = 0, dense_levels = 0;
   int diam = 1, disconnected = 0, windows = 0;
   bool adj_ok = true;
 
@@ -162,125 +678,159 @@ __global__ void __launch_bounds__(kThreads, 2) apsp_persistent_kernel(const Apsp
     if (nsrc <= 0) continue;
     const int row0 = phase == 1 ? 0 : N - a.ac;
     const int nwin = (nsrc + W - 1) / W;
-    for (int t = a.win_first; t < nwin && !disconnected; t += a.win_stride) {
+    const bool use_ball = phase == 1 && a.ball != nullptr;
+    int local = 0;
+    for (int t = a.win_first; t < nwin && !disconnected; t += a.win_stride, ++local) {
       const int first = t * W;
       const int l = min(W, nsrc - first);
       const long long lo_rows = a.split, hi_rows = (long long)N - a.split;
+      const int base = row0 + first;   // vertex id of the window's bit 0
       ++windows;
 
-      // Window start: both matrices hold the identity (reference :168-172):
-      // bit i of row row0+first+i for i < l, every other bit zero.
-      for (long long v = slot; v < N; v += n_slots) {
-        const long long bit = v - row0 - first;
-#pragma unroll
-        for (int k = 0; k < UPL; ++k) {
-          const int col = li + k * LPR;      // uint4 index within the row
-          uint4 x = make_uint4(0u, 0u, 0u, 0u);
-          if (bit >= 0 && bit < l && (int)(bit >> 7) == col) {
-            const unsigned b = (unsigned)(bit & 127);
-            const unsigned m = 1u << (b & 31);
-            if ((b >> 5) == 0) x.x = m; else if ((b >> 5) == 1) x.y = m;
-            else if ((b >> 5) == 2) x.z = m; else x.w = m;
-          }
-          st_cg(a.buf0 + v * R + col, x);
-          st_cg(a.buf1 + v * R + col, x);
+      long long prev_total = l;   // popcount of the identity S_0
+      long long kk = 0;
+      int act = 0;
+      const uint4* cur;           // S_kk rows the next sweep gathers from
+      uint4* nxt;                 // rows it writes
+      bool own_count = false;     // the first sweep of a ball window also reports S_3
+      if (use_ball) {
+        // ---- levels 0 and 1 from the ball pre-pass; S_3 rows are in HBM --------
+        const unsigned long long* bc = a.ball_cnt + (size_t)local * 6;
+        for (kk = 0; kk < 2; ++kk) {
+          ++levels;
+          act = level_decision(phase, (long long)__ldcg(bc + 2 * kk), (long long)__ldcg(bc + 2 * kk + 1), l, N,
+                               lo_rows, hi_rows, a.groups, prev_total, sum);
+          if (act) break;
         }
-      }
-      bar_target += grid;
-      if (!grid_barrier(a.ctrl, bar_target + a.phantom, a.timeout_ns, &s_flag)) return;
-
-      long long prev_total = l;   // popcount of the identity
-      long long kk;
-      for (kk = 0; kk < N; ++kk) {
-        const uint4* __restrict__ src = (kk & 1) ? a.buf1 : a.buf0;
-        uint4* __restrict__ dst = (kk & 1) ? a.buf0 : a.buf1;
-        unsigned c_lo = 0, c_hi = 0;
-        for (long long v = slot; v < N; v += n_slots) {
-          const int* arow = a.adj + v * d;
-          uint4 acc[UPL];
-#pragma unroll
-          for (int k = 0; k < UPL; ++k) acc[k] = ld_cg(dst + v * R + li + k * LPR);
-          int j = 0;
-          for (; j + U <= d; j += U) {
-            int u[U];
-#pragma unroll
-            for (int q = 0; q < U; ++q) u[q] = __ldg(arow + j + q);
-#pragma unroll
-            for (int q = 0; q < U; ++q) {
-              if ((unsigned)u[q] >= (unsigned)N) { adj_ok = false; u[q] = 0; }
-            }
-            uint4 x[U][UPL];
-#pragma unroll
-            for (int q = 0; q < U; ++q)
-#pragma unroll
-              for (int k = 0; k < UPL; ++k) x[q][k] = ld_cg(src + (long long)u[q] * R + li + k * LPR);
-#pragma unroll
-            for (int q = 0; q < U; ++q)
-#pragma unroll
-              for (int k = 0; k < UPL; ++k) or_into(acc[k], x[q][k]);
-          }
-          for (; j < d; ++j) {
-            int u = __ldg(arow + j);
-            if ((unsigned)u >= (unsigned)N) { adj_ok = false; u = 0; }
-#pragma unroll
-            for (int k = 0; k < UPL; ++k) or_into(acc[k], ld_cg(src + (long long)u * R + li + k * LPR));
-          }
-          unsigned c = 0;
-#pragma unroll
-          for (int k = 0; k < UPL; ++k) {
-            st_cg(dst + v * R + li + k * LPR, acc[k]);
-            c += popc4(acc[k]);
-          }
-          if (v < a.split) c_lo += c; else c_hi += c;
-        }
+        if (!act) kk = 3;
+        own_count = true;
+        cur = a.ball + (size_t)local * N * R;
+        nxt = a.buf0;
+      } else {
+        // ---- levels 0 and 1 by two-hop seeding into buf0 -----------------------
+        unsigned c[4] = {0u, 0u, 0u, 0u};  // S_1 lo, S_1 hi, S_2 lo, S_2 hi
+        if (a.vec4)
+          seed_window<R, 4>(a, base, l, a.buf0, my_nb, my_rows, c, adj_ok, warp_id, n_warps);
+        else
+          seed_window<R, 1>(a, base, l, a.buf0, my_nb, my_rows, c, adj_ok, warp_id, n_warps);
         if (!adj_ok) set_error(a.ctrl, kErrAdj, (int)blockIdx.x);
-
-        // CTA reduction of the level's popcounts, one atomic per CTA.
-        unsigned long long r_lo = c_lo, r_hi = c_hi;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-          r_lo += __shfl_xor_sync(0xffffffffu, r_lo, o);
-          r_hi += __shfl_xor_sync(0xffffffffu, r_hi, o);
-        }
-        if (lane == 0) { s_red[warp][0] = r_lo; s_red[warp][1] = r_hi; }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-          unsigned long long b_lo = 0, b_hi = 0;
-#pragma unroll
-          for (int w = 0; w < kWarps; ++w) { b_lo += s_red[w][0]; b_hi += s_red[w][1]; }
-          if (b_lo) atomicAdd(&a.ctrl->cnt[gl & 1][0], b_lo);
-          if (b_hi) atomicAdd(&a.ctrl->cnt[gl & 1][1], b_hi);
-        }
+        cta_add_counts<4>(c, a.ctrl, gl, s_red);
         bar_target += grid;
         if (!grid_barrier(a.ctrl, bar_target + a.phantom, a.timeout_ns, &s_flag)) return;
-        if (threadIdx.x == 0) {
-          s_cnt[0] = ld_acquire_u64(&a.ctrl->cnt[gl & 1][0]);
-          s_cnt[1] = ld_acquire_u64(&a.ctrl->cnt[gl & 1][1]);
-        }
+        trace_mark(a, ntrace, 1, 1);
+        read_level_counts(a.ctrl, gl, 2, s_seen, s_lvl);
+        const long long seed_lvl[4] = {s_lvl[0], s_lvl[1], s_lvl[2], s_lvl[3]};
         __syncthreads();
-        const unsigned long long now_lo = s_cnt[0], now_hi = s_cnt[1];
-        __syncthreads();   // s_cnt is rewritten after the next barrier only
-        const long long lvl_lo = (long long)(now_lo - seen[gl & 1][0]);
-        const long long lvl_hi = (long long)(now_hi - seen[gl & 1][1]);
-        seen[gl & 1][0] = now_lo;
-        seen[gl & 1][1] = now_hi;
-        ++gl;
+        if (ld_volatile_i32(&a.ctrl->error) != 0) return;
+        gl += 2;
         ++levels;
-        if (ld_volatile_i32(&a.ctrl->error) != 0) return;   // same answer in every CTA after the barrier
-
-        const long long total = lvl_lo + lvl_hi;
-        const bool full = phase == 1 ? (total == (long long)N * l) : (lvl_hi == hi_rows * l);
-        if (full) break;
-        if (total == prev_total) { disconnected = 1; break; }
-        if (phase == 1) {
-          sum += (lo_rows * l - lvl_lo) * a.groups;
-          sum += (hi_rows * l - lvl_hi) * 2LL * a.groups;
-        } else {
-          sum += hi_rows * l - lvl_hi;
+        act = level_decision(phase, seed_lvl[0], seed_lvl[1], l, N, lo_rows, hi_rows, a.groups, prev_total, sum);
+        if (!act) {
+          kk = 1;
+          ++levels;
+          act = level_decision(phase, seed_lvl[2], seed_lvl[3], l, N, lo_rows, hi_rows, a.groups, prev_total,
+                               sum);
         }
-        prev_total = total;
+        if (!act) kk = 2;
+        cur = a.buf0;
+        nxt = a.buf1;
       }
-      if (disconnected) diam = N + 1;
+      if (!act) {
+        // ---- dense OR-gather sweeps ------------------------------------------------
+        for (; kk < N; ++kk) {
+          const uint4* __restrict__ src = cur;
+          uint4* __restrict__ dst = nxt;
+          unsigned cl[4] = {0u, 0u, 0u, 0u};   // new rows lo/hi, then (own_count) own rows lo/hi
+          // The skipping sweep pays once the gathered level is nearly full
+          // (its count, prev_total, is known); on denser-to-come levels the
+          // plain sweep is faster.
+          bool wide = false;
+          if constexpr (LPR == 32) {
+            if (d <= 32 && !own_count && prev_total * 10 >= (long long)N * l * 9) {
+              wide = true;
+              sweep_wide<R>(src, dst, a.adj, N, d, a.split, slot, n_slots, l, own_count, cl, adj_ok);
+            }
+          }
+          for (long long v = wide ? N : slot; v < N; v += n_slots) {
+            const int* arow = a.adj + v * d;
+            uint4 acc[UPL];
+#pragma unroll
+            for (int k = 0; k < UPL; ++k) acc[k] = ld_cg(src + v * R + li + k * LPR);
+            if (own_count) {
+              unsigned co = 0;
+#pragma unroll
+              for (int k = 0; k < UPL; ++k) co += popc4(acc[k]);
+              if (v < a.split) cl[2] += co; else cl[3] += co;
+            }
+            int j = 0;
+            for (; j + U <= d; j += U) {
+              int u[U];
+#pragma unroll
+              for (int q = 0; q < U; ++q) u[q] = __ldg(arow + j + q);
+#pragma unroll
+              for (int q = 0; q < U; ++q) {
+                if ((unsigned)u[q] >= (unsigned)N) { adj_ok = false; u[q] = 0; }
+              }
+              uint4 x[U][UPL];
+#pragma unroll
+              for (int q = 0; q < U; ++q)
+#pragma unroll
+                for (int k = 0; k < UPL; ++k) x[q][k] = ld_cg(src + (long long)u[q] * R + li + k * LPR);
+#pragma unroll
+              for (int q = 0; q < U; ++q)
+#pragma unroll
+                for (int k = 0; k < UPL; ++k) or_into(acc[k], x[q][k]);
+            }
+            for (; j < d; ++j) {
+              int u = __ldg(arow + j);
+              if ((unsigned)u >= (unsigned)N) { adj_ok = false; u = 0; }
+#pragma unroll
+              for (int k = 0; k < UPL; ++k) or_into(acc[k], ld_cg(src + (long long)u * R + li + k * LPR));
+            }
+            unsigned cc = 0;
+#pragma unroll
+            for (int k = 0; k < UPL; ++k) {
+              st_cg(dst + v * R + li + k * LPR, acc[k]);
+              cc += popc4(acc[k]);
+            }
+            if (v < a.split) cl[0] += cc; else cl[1] += cc;
+          }
+          if (!adj_ok) set_error(a.ctrl, kErrAdj, (int)blockIdx.x);
+          if (own_count) {
+            // slot gl: S_kk (own rows, level kk-1); slot gl+1: S_kk+1 (level kk)
+            const unsigned c4[4] = {cl[2], cl[3], cl[0], cl[1]};
+            cta_add_counts<4>(c4, a.ctrl, gl, s_red);
+          } else {
+            cta_add_counts<2>(cl, a.ctrl, gl, s_red);
+          }
+          bar_target += grid;
+          if (!grid_barrier(a.ctrl, bar_target + a.phantom, a.timeout_ns, &s_flag)) return;
+          trace_mark(a, ntrace, 2, kk);
+          read_level_counts(a.ctrl, gl, own_count ? 2 : 1, s_seen, s_lvl);
+          const long long l0 = s_lvl[0], l1 = s_lvl[1], l2 = s_lvl[2], l3 = s_lvl[3];
+          __syncthreads();   // s_lvl is rewritten after the next barrier only
+          if (ld_volatile_i32(&a.ctrl->error) != 0) return;   // same answer in every CTA after the barrier
+          ++dense_levels;
+          if (own_count) {
+            ++gl;
+            ++levels;
+            act = level_decision(phase, l0, l1, l, N, lo_rows, hi_rows, a.groups, prev_total, sum);
+            if (act) { --kk; ++gl; break; }   // complete (or stalled) at S_kk: this sweep was not needed
+            own_count = false;
+            ++gl;
+            ++levels;
+            act = level_decision(phase, l2, l3, l, N, lo_rows, hi_rows, a.groups, prev_total, sum);
+          } else {
+            ++gl;
+            ++levels;
+            act = level_decision(phase, l0, l1, l, N, lo_rows, hi_rows, a.groups, prev_total, sum);
+          }
+          if (act) break;
+          cur = dst;
+          nxt = (dst == a.buf0) ? a.buf1 : a.buf0;
+        }
+      }
+      if (act == 2) { disconnected = 1; diam = N + 1; }
       else if (kk + 1 > diam) diam = (int)(kk + 1);
     }
   }
@@ -291,10 +841,18 @@ __global__ void __launch_bounds__(kThreads, 2) apsp_persistent_kernel(const Apsp
     c->disconnected = disconnected;
     c->sum = sum;
     c->levels = levels;
+    c->dense_levels = dense_levels;
     c->windows = windows;
+    c->trace_len = ntrace;
     __threadfence();
     c->done = 1;
   }
+}
+
+// Shared memory the persistent kernel needs for its seeding rows, in bytes.
+template <int R>
+constexpr size_t apsp_smem_bytes() {
+  return (size_t)kWarps * (kSeedVerts * kSeedNb + 2 * kSeedVerts * 4 * R) * sizeof(unsigned);
 }
 
 // Grid relabel (grid/evaluation.c:148-151): row rotate_hash[i] of the

@@ -40,11 +40,12 @@ class Result:
     levels: int         # BFS levels executed over all source windows
     windows: int
     window_bits: int
+    dense_levels: int   # of which dense OR-gather sweeps
 
     @staticmethod
     def from_c(r: ggb_result) -> "Result":
         return Result(bool(r.connected), int(r.diameter), float(r.aspl), int(r.total), int(r.levels),
-                      int(r.windows), int(r.window_bits))
+                      int(r.windows), int(r.window_bits), int(r.dense_levels))
 
 
 def _raise(rc: int) -> None:
@@ -123,7 +124,7 @@ def evaluate_partial(adj, rank: int, procs: int, based_nodes: int | None = None,
 
 def finish_general(nodes: int, diam: int, disconnected: int, total_sum: int) -> Result:
     """Completes all-reduced partials (MAX diam, MAX disconnected, SUM sum)."""
-    p = ggb_partial(diam, disconnected, total_sum, 0, 0, 0)
+    p = ggb_partial(diam, disconnected, total_sum, 0, 0, 0, 0)
     r = ggb_result()
     _raise(load().ggb_finish_general(nodes, C.byref(p), C.byref(r)))
     return Result.from_c(r)
@@ -132,6 +133,11 @@ def finish_general(nodes: int, diam: int, disconnected: int, total_sum: int) -> 
 def set_tuning(window_bits: int = 0, ctas: int = 0) -> None:
     """Forces the source-window width / grid size (0 = automatic)."""
     _raise(load().ggb_set_tuning(window_bits, ctas))
+
+
+def set_ball(mode: int = -1) -> None:
+    """Ball pre-pass policy: -1 automatic, 0 never, 1 whenever feasible."""
+    _raise(load().ggb_set_ball(mode))
 
 
 def kernel_launches() -> int:

@@ -52,6 +52,9 @@ typedef struct ggb_result {
   long long levels;     /* BFS levels executed, summed over source windows   */
   int windows;          /* source windows run                                 */
   int window_bits;      /* sources per window (a multiple of 128)             */
+  long long dense_levels; /* of `levels`, those run as dense OR-gather sweeps
+                           (the first two levels of a window are seeded from
+                           the two-hop adjacency instead)                     */
 } ggb_result;
 
 /* Partial result of a rank that ran a strided share of the source windows
@@ -64,6 +67,7 @@ typedef struct ggb_partial {
   long long levels;
   int windows;
   int window_bits;
+  long long dense_levels;
 } ggb_partial;
 
 /* ---- lifecycle --------------------------------------------------------- */
@@ -91,12 +95,30 @@ int ggb_device_count(void);
  * by tests that sweep widths; results never depend on either. */
 int ggb_set_tuning(int window_bits, int ctas);
 
+/* Policy for the ball pre-pass (one kernel that writes S_3 of every source
+ * window, so that windows start their dense sweeps at level 3): -1 automatic
+ * by the cost model, 0 never, 1 whenever the sizes allow it (degree <= 32,
+ * at most 64 windows per rank, the row fits in shared memory).  Results
+ * never depend on it. */
+int ggb_set_ball(int mode);
+
 /* Test hook for the bounded device waits: every grid-barrier wait gives up
  * after timeout_ns, and `phantom` extra arrivals that never come are added to
  * every barrier.  phantom=1 makes each wait run out, which must surface as
  * GGB_ETIMEOUT with the CUDA context still usable.  (2e9, 0) restores the
  * default. */
 int ggb_set_barrier_test(long long timeout_ns, int phantom);
+
+/* Opt-in timeline of the persistent kernel: with capacity > 0, CTA 0 records
+ * a (globaltimer ns, tag | level << 8) pair after every grid barrier of the
+ * following evaluations (tag 1: a window's two seeded levels, tag 2: a dense
+ * sweep).  0 turns it off.  The device-side analogue of the reference's
+ * TIMER_APSP bracket (general/timer.c), one level finer. */
+int ggb_trace_enable(int capacity);
+
+/* Copies the last evaluation's trace pairs to out (2*max_pairs long longs);
+ * returns the number of pairs copied. */
+int ggb_trace_read(long long *out, int max_pairs);
 
 /* ---- host-buffer entry points (copy in, evaluate, copy out) ------------ */
 

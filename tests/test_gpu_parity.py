@@ -133,3 +133,42 @@ def test_large_properties(gpu):
             r = _gpu(c, adj, rh)
             assert (r.diameter, r.total) == (c["expected"]["diameter"], c["expected"]["total"])
             assert r.windows == -(-65536 // c["groups"] // r.window_bits)
+
+
+@pytest.mark.parametrize("ball", [0, 1])
+@pytest.mark.parametrize("bits", [128, 1024, 4096])
+@pytest.mark.parametrize("n,d,g,ac", [(3000, 7, 1, 0), (3000, 8, 1, 0), (2400, 12, 4, 0), (1040, 8, 16, 16),
+                                      (5000, 5, 1, 100), (700, 32, 1, 0)])
+def test_seeding_paths(gpu, ball, bits, n, d, g, ac):
+    """Both ways of starting a window -- the per-window two-hop seeding and
+    the ball pre-pass -- with scalar (odd degree) and vector adjacency loads,
+    over one and many windows, give the oracle's answer."""
+    adj = graphs.random_regular(n, d, n + d + g).adj
+    bn = (n - ac) // g
+    want = oracle.general(adj, based_nodes=bn, groups=g, added_centers=ac)
+    try:
+        gg.set_ball(ball)
+        gg.set_tuning(bits, 0)
+        r = gg.evaluate(adj, based_nodes=bn, groups=g, added_centers=ac)
+    finally:
+        gg.set_ball(-1)
+        gg.set_tuning(0, 0)
+    assert (r.connected, r.diameter, r.aspl, r.total) == want
+
+
+@pytest.mark.parametrize("ball", [0, 1])
+def test_seeding_paths_grid_and_disconnected(gpu, ball):
+    try:
+        gg.set_ball(ball)
+        gg.set_tuning(256, 0)
+        gr = graphs.grid_regular(30, 30, 4, 3, 5)
+        rh = graphs.rotate_hash(gr.nodes, 30, 30, 2)
+        want = oracle.grid(gr.adj, rh, groups=2)
+        res = gg.evaluate_grid(gr.adj, rh, groups=2)
+        assert (res.connected, res.diameter, res.aspl, res.total) == want
+        adj = union_graph(900, 6, 5)
+        r = gg.evaluate(adj)
+        assert (r.connected, r.diameter, r.aspl) == oracle.general(adj)[:3]
+    finally:
+        gg.set_ball(-1)
+        gg.set_tuning(0, 0)
