@@ -73,6 +73,9 @@ CORE_SIGNATURES = {
     "ggb_eval_general_partial": (_I, [_I, _I, _I, _I, _P, _I, _I, _I, C.POINTER(ggb_partial)]),
     "ggb_finish_general": (_I, [_I, C.POINTER(ggb_partial), C.POINTER(ggb_result)]),
     "ggb_finish_grid": (_I, [_I, C.POINTER(ggb_partial), C.POINTER(ggb_result)]),
+    "ggb_eval_general_noalloc": (_I, [_I, _I, _I, _I, _P, _I, _P, C.POINTER(ggb_result)]),
+    "ggb_noalloc_scratch_bytes": (_LL, []),
+    "ggb_noalloc_last_error": (C.c_char_p, []),
 }
 
 HOST_SIGNATURES = {

@@ -25,6 +25,46 @@
 #include "../../include/graphgolf_b200.h"
 #include "apsp_kernel.cuh"
 
+namespace ggb {
+
+// Grid relabel (grid/evaluation.c:148-151): row rotate_hash[i] of the
+// relabelled adjacency holds rotate_hash[adj[i][j]].  inv[] must be -1 on
+// entry; it receives the inverse permutation so a second kernel can verify
+// that rotate_hash is a bijection.
+__global__ void relabel_adjacency_kernel(const int* __restrict__ adj, const int* __restrict__ rh,
+                                         int* __restrict__ out, int* __restrict__ inv, int N, int d,
+                                         ApspCtrl* ctrl) {
+  const long long n = (long long)N * d;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(e / d), j = (int)(e % d);
+    const int r = rh[i];
+    const int nb = adj[e];
+    if ((unsigned)r >= (unsigned)N) { set_error(ctrl, kErrPerm, i); continue; }
+    if ((unsigned)nb >= (unsigned)N) { set_error(ctrl, kErrAdj, i); continue; }
+    const int rn = rh[nb];
+    if ((unsigned)rn >= (unsigned)N) { set_error(ctrl, kErrPerm, nb); continue; }
+    out[(long long)r * d + j] = rn;
+    if (j == 0) inv[r] = i;
+  }
+  if (d == 0) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N;
+         i += (long long)gridDim.x * blockDim.x) {
+      const int r = rh[i];
+      if ((unsigned)r >= (unsigned)N) { set_error(ctrl, kErrPerm, (int)i); continue; }
+      inv[r] = (int)i;
+    }
+  }
+}
+
+__global__ void check_permutation_kernel(const int* __restrict__ inv, int N, ApspCtrl* ctrl) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N;
+       i += (long long)gridDim.x * blockDim.x)
+    if (inv[i] < 0) set_error(ctrl, kErrPerm, (int)i);
+}
+
+}  // namespace ggb
+
 namespace {
 
 using ggb::ApspArgs;

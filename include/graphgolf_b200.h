@@ -158,6 +158,30 @@ int ggb_collect(void *stream, ggb_result *out);
  * one persistent kernel plus, for grids, two relabel kernels). */
 long long ggb_kernel_launches(void);
 
+/* ---- evaluation without device allocation ------------------------------- */
+
+/* No counterpart in the reference.  For callers that cannot let a library
+ * call cudaMalloc -- a host whose device memory belongs to another allocator
+ * (a framework's caching pool, a fixed budget carved out at start-up) or an
+ * annealing loop that must not allocate while it runs.  Same result as
+ * ggb_eval_general_device; allocates nothing: the kernel's scratch lives in a
+ * 16 MiB file-scope device array (ggb_noalloc_scratch_bytes()) that every GPU
+ * loading this library holds until exit, so nodes must be at most 524280
+ * (larger graphs are rejected with GGB_EINVAL).  adj_dev is a device pointer,
+ * `out` a host pointer; the call waits for its result on `stream` (NULL: the
+ * default stream).  The first call on a device looks up the array's device
+ * address; make it before any stream capture.  All calls share the one array:
+ * calls that overlap on the GPU (two threads or two streams) race and must be
+ * serialised by the caller. */
+int ggb_eval_general_noalloc(int nodes, int based_nodes, int groups, int degree, const int *adj_dev,
+                             int added_centers, void *stream, ggb_result *out);
+
+/* Size in bytes of the device array ggb_eval_general_noalloc works in. */
+long long ggb_noalloc_scratch_bytes(void);
+
+/* Text of the last error of ggb_eval_general_noalloc ("" if none). */
+const char *ggb_noalloc_last_error(void);
+
 /* ---- multi-rank decomposition (one GPU per rank) ------------------------ */
 
 /* Runs only the source windows t = rank, rank+procs, ... of a general graph
