@@ -1,0 +1,82 @@
+"""Drop-in check: the reference's own host programs (main/sa/common/timer of
+general/ and grid/, compiled from their sources into oracle/_ref) linked
+against this repository's libgg_general.so / libgg_grid.so instead of the
+reference evaluation.o, against the same programs linked with the
+reference's CPU evaluator.  For the same seed the whole simulated-annealing
+run must be identical: every progress row (current/best ASPL and diameter,
+accept counts -- the accept/reject trajectory), the final result and the
+written graph.  Only lines with wall-clock times or host names differ."""
+import subprocess
+from pathlib import Path
+
+import pytest
+
+import oracle
+from graphgolf_b200 import graphs
+
+pytestmark = pytest.mark.gpu
+
+REF = oracle.REF_DIR
+
+
+def _need(*names):
+    for n in names:
+        if not (REF / n).exists():
+            pytest.skip(f"oracle/_ref/{n} not built (reference sources absent at build time)")
+
+
+def _stable(text: str):
+    drop = ("Run on", "sec", "---", "Seed", "Num. of threads", "Processes", "Num. of processes", "Output filename")
+    out = []
+    for line in text.splitlines():
+        if any(k in line for k in drop):
+            continue
+        if line[:3] in ("Mon", "Tue", "Wed", "Thu", "Fri", "Sat", "Sun"):
+            continue
+        out.append(line.rstrip())
+    return out
+
+
+def _run(binary, args, cwd):
+    p = subprocess.run([str(REF / binary), *args], cwd=cwd, capture_output=True, text=True, timeout=600)
+    assert p.returncode == 0, p.stdout[-2000:] + p.stderr[-2000:]
+    return p.stdout
+
+
+@pytest.mark.parametrize("n,d,g,seed,steps", [(1024, 8, 1, 1, 1000), (512, 6, 8, 3, 800), (2048, 12, 16, 5, 400)])
+def test_general_sa_trajectory_identical(gpu, tmp_path, n, d, g, seed, steps):
+    _need("gg", "gg_b200")
+    gr = graphs.symmetric_regular(n, d, g, seed) if g > 1 else graphs.random_regular(n, d, seed)
+    f = tmp_path / "in.edges"
+    graphs.write_general(str(f), gr)
+    args = ["-f", str(f), "-M", "-g", str(g), "-s", str(seed), "-n", str(steps)]
+    cpu = _run("gg", args + ["-o", str(tmp_path / "cpu.edges")], tmp_path)
+    gpu_out = _run("gg_b200", args + ["-o", str(tmp_path / "gpu.edges")], tmp_path)
+    a, b = _stable(cpu), _stable(gpu_out)
+    assert any("Diam. k" in l for l in a)
+    assert a == b
+    assert (tmp_path / "cpu.edges").read_text() == (tmp_path / "gpu.edges").read_text()
+
+
+def test_general_startup_randomisation_identical(gpu, tmp_path):
+    """Without -M the reference first randomises the graph with 2-opt moves
+    until evaluation() reports it connected (general/main.c:193-207)."""
+    _need("gg", "gg_b200")
+    gr = graphs.random_regular(256, 4, 9)
+    f = tmp_path / "in.edges"
+    graphs.write_general(str(f), gr)
+    args = ["-f", str(f), "-s", "2", "-n", "300"]
+    assert _stable(_run("gg", args, tmp_path)) == _stable(_run("gg_b200", args, tmp_path))
+
+
+@pytest.mark.parametrize("w,h,d,r,seed,steps", [(20, 20, 4, 3, 1, 400), (30, 30, 6, 3, 2, 200)])
+def test_grid_sa_trajectory_identical(gpu, tmp_path, w, h, d, r, seed, steps):
+    _need("gg_grid", "gg_grid_b200")
+    gr = graphs.grid_regular(w, h, d, r, seed)
+    f = tmp_path / "in.edges"
+    graphs.write_grid(str(f), gr)
+    args = ["-f", str(f), "-R", str(r), "-s", str(seed), "-n", str(steps)]
+    cpu = _run("gg_grid", args + ["-o", str(tmp_path / "cpu.edges")], tmp_path)
+    gpu_out = _run("gg_grid_b200", args + ["-o", str(tmp_path / "gpu.edges")], tmp_path)
+    assert _stable(cpu) == _stable(gpu_out)
+    assert (tmp_path / "cpu.edges").read_text() == (tmp_path / "gpu.edges").read_text()
