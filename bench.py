@@ -12,9 +12,12 @@ total, ASPL) of that graph.
 * ``e2e``    -- the same metric through the public C ABI with host buffers
   (ggb_eval_general: pinned staging, H2D of the adjacency, kernel, D2H of the
   result block, synchronise), wall-clock per call.
-* ``roofline`` -- algorithmic bytes of the kernel (per executed window-level:
-  N*d*4 adjacency + N*d*W/8 gathered rows + N*W/8 own row read + N*W/8 write)
-  over its event-timed duration, against the measured HBM copy bandwidth.
+* ``roofline`` -- the dominant kernel (the persistent sweep kernel): its
+  algorithmic bytes (per dense sweep: N*d*4 adjacency + N*d*W/8 gathered rows
+  + N*W/8 own row read + N*W/8 write) over its own event-timed duration
+  (events recorded by the library on the launching stream), against the
+  measured HBM copy bandwidth, and against the measured random-row L2 gather
+  rate (ggb_probe_l2_gather), the roof an L2-resident sweep meets.
 * ``cpu_baseline`` -- the reference's own OpenMP evaluator (compiled from its
   sources into oracle/_ref) on this host's cores, over a bounded sample.
 
@@ -33,9 +36,7 @@ import ctypes as C
 import json
 import os
 import statistics
-import subprocess
 import sys
-import tempfile
 import time
 from pathlib import Path
 
@@ -74,65 +75,75 @@ def _graph(wl: dict, rank: int):
 
 
 class Clocks:
-    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+    """Samples SM clocks and throttle reasons during the timed region: NVML
+    read in a background thread every 10 ms (reads only; nothing is set)."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40,
+               "sw_power_cap": 0x4}
 
     def __init__(self, index: int):
         self.index = index
-        self.proc = None
-        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.samples = []
+        self.max_mhz = None
+        self._stop = None
+        self._thread = None
+        self.err = None
 
     def __enter__(self):
+        import threading
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
-                                         stdout=self.f, stderr=subprocess.DEVNULL)
-        except (OSError, ValueError):
-            self.proc = None
+            import pynvml
+            pynvml.nvmlInit()
+            h = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+        except Exception as e:  # no NVML: report it, never invent a sample
+            self.err = f"nvml unavailable: {type(e).__name__}"
+            return self
+        self._stop = threading.Event()
+
+        def run():
+            while not self._stop.is_set():
+                try:
+                    mhz = pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)
+                    rs = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+                    self.samples.append((mhz, rs))
+                except Exception:
+                    pass
+                self._stop.wait(0.01)
+
+        self._thread = threading.Thread(target=run, daemon=True)
+        self._thread.start()
         return self
 
     def __exit__(self, *a):
-        if self.proc:
-            self.proc.terminate()
-            try:
-                self.proc.wait(timeout=5)
-            except subprocess.TimeoutExpired:
-                self.proc.kill()
+        if self._thread:
+            self._stop.set()
+            self._thread.join(timeout=2)
 
     def summary(self):
-        if not self.proc:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.f.flush()
-        rows = [l.split(",") for l in Path(self.f.name).read_text().splitlines() if l.strip()]
-        sm, mx, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for r in rows:
-            r = [x.strip() for x in r]
-            try:
-                sm.append(float(r[1]))
-                mx.append(float(r[2]))
-            except (ValueError, IndexError):
-                continue
-            for k, name in enumerate(names):
-                if len(r) > 5 + k and r[5 + k].lower() == "active":
-                    reasons.add(name)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": [self.err or "no samples"],
+                    "samples": 0}
+        mhz = [m for m, _ in self.samples]
+        reasons = sorted({k for _, r in self.samples for k, bit in self.REASONS.items() if r & bit})
+        return {"sm_mhz": statistics.median(mhz), "sm_max_mhz": self.max_mhz, "reasons": reasons,
+                "samples": len(mhz)}
 
 
-def algorithmic_bytes(nodes: int, degree: int, dense_levels: int, windows: int, window_bits: int) -> int:
-    """Bytes one evaluation must move.  Per dense sweep of a window: the
-    adjacency (N*d*4), the d gathered rows of every vertex (N*d*W/8), its own
-    row read and the new row written (2*N*W/8).  Per window, the seeding of
-    the first two levels: the two-hop adjacency (N*(d+d^2)*4) and two rows
-    written (2*N*W/8)."""
+def sweep_bytes(nodes: int, degree: int, dense_levels: int, window_bits: int) -> int:
+    """Algorithmic bytes of the persistent kernel per launch: per dense sweep,
+    the adjacency (N*d*4), the d gathered rows of every vertex (N*d*W/8), its
+    own row read and the new row written (2*N*W/8) -- the per-level figure of
+    the bit-parallel BFS with W-bit rows."""
     row = window_bits // 8
-    dense = dense_levels * (nodes * degree * 4 + nodes * degree * row + 2 * nodes * row)
-    seed = windows * (nodes * (degree + degree * degree) * 4 + 2 * nodes * row)
-    return dense + seed
+    return dense_levels * (nodes * degree * 4 + nodes * degree * row + 2 * nodes * row)
+
+
+def ball_bytes(nodes: int, degree: int, windows: int, window_bits: int) -> int:
+    """Algorithmic bytes of the ball pre-pass: the 1 + d + d^2 + d^3 adjacency
+    entries of every vertex's three-hop ball read, and its S_3 row of every
+    window written out."""
+    return nodes * (1 + degree + degree ** 2 + degree ** 3) * 4 + windows * nodes * window_bits // 8
 
 
 def survey_formula_bytes(nodes: int, degree: int, levels: int, window_bits: int) -> int:
@@ -281,6 +292,8 @@ def main() -> int:
     for _ in range(args.warmup):
         one()
     first = gg.Result.from_c(res)
+    lib.ggb_set_timing(1)
+    kt_ball, kt_pers = [], []
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     launches0 = lib.ggb_kernel_launches()
     if dist:
@@ -290,7 +303,12 @@ def main() -> int:
         for k in range(args.steps):
             one(evs[k])
             assert res.total == first.total and res.diameter == first.diameter
+            mb, mp = C.c_double(0), C.c_double(0)
+            if lib.ggb_kernel_times(C.byref(mb), C.byref(mp)) == 0:
+                kt_ball.append(mb.value)
+                kt_pers.append(mp.value)
         torch.cuda.synchronize()
+    lib.ggb_set_timing(0)
     if dist:
         dist.barrier()
     launches = lib.ggb_kernel_launches() - launches0
@@ -323,12 +341,19 @@ def main() -> int:
     e2e_value = world * args.steps / e2e_max
 
     peak, peak_kind = _peaks()
-    alg = algorithmic_bytes(n, d, first.dense_levels, first.windows, first.window_bits)
-    achieved = alg / (mean_ms / 1e3) / 1e9
-    traffic = None
-    tp = ROOT / "profiles" / f"apsp_{args.workload}_dram.json"
+    # dominant kernel: the persistent kernel (dense sweeps); the ball pre-pass is reported beside it
+    pers_ms = statistics.mean(kt_pers) if kt_pers else mean_ms
+    ball_ms = statistics.mean(kt_ball) if kt_ball else 0.0
+    alg = sweep_bytes(n, d, first.dense_levels, first.window_bits)
+    achieved = alg / (pers_ms / 1e3) / 1e9
+    l2_peak = C.c_double(0)
+    l2_ok = lib.ggb_probe_l2_gather(n, d, first.window_bits, 20, C.byref(l2_peak)) == 0
+    prof = {}
+    tp = ROOT / "profiles" / f"apsp_{args.workload}_traffic.json"
     if tp.exists():
-        traffic = json.loads(tp.read_text()).get("dram_bytes_per_launch")
+        prof = json.loads(tp.read_text())
+    traffic = prof.get("apsp_persistent_kernel", {}).get("dram_bytes_per_launch")
+    lts = prof.get("apsp_persistent_kernel", {}).get("lts_bytes_per_launch")
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": mean_ms, "higher_is_better": True, "scaling": "weak",
@@ -342,11 +367,21 @@ def main() -> int:
                        "parallelism": f"independent graph per rank x{world}"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
+                         "kernel": f"apsp_persistent_kernel<{first.window_bits // 128}>",
+                         "ms_per_launch": pers_ms,
                          "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured"
                          else "fallback 6650 GB/s",
                          "algorithmic_bytes_per_launch": alg,
-                         "survey_formula_bytes_per_launch": survey_formula_bytes(n, d, first.levels,
-                                                                                 first.window_bits)},
+                         "l2_gather_peak_gbs": l2_peak.value if l2_ok else None,
+                         "frac_of_l2_gather_peak": (achieved / l2_peak.value) if l2_ok and l2_peak.value else None,
+                         "lts_bytes_per_launch": lts,
+                         "note": "the window working set is L2-resident by design; traffic = DRAM bytes per "
+                                 "launch from the committed ncu capture under profiles/"},
+            "ball_prepass": {"ms_per_launch": ball_ms,
+                             "algorithmic_bytes_per_launch": ball_bytes(n, d, first.windows, first.window_bits)
+                             if ball_ms else 0,
+                             "traffic": prof.get("ball_kernel", {}).get("dram_bytes_per_launch")},
+            "survey_formula_bytes_per_eval": survey_formula_bytes(n, d, first.levels, first.window_bits),
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": n * d * 4,
                     "d2h_bytes_per_step": 96},
             "gpu_launches": int(launches),

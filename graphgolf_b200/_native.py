@@ -69,6 +69,9 @@ CORE_SIGNATURES = {
     "ggb_collect": (_I, [_P, C.POINTER(ggb_result)]),
     "ggb_kernel_launches": (_LL, []),
     "ggb_trace_enable": (_I, [_I]),
+    "ggb_set_timing": (_I, [_I]),
+    "ggb_kernel_times": (_I, [C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "ggb_probe_l2_gather": (_I, [_I, _I, _I, _I, C.POINTER(C.c_double)]),
     "ggb_trace_read": (_I, [_P, _I]),
     "ggb_eval_general_partial": (_I, [_I, _I, _I, _I, _P, _I, _I, _I, C.POINTER(ggb_partial)]),
     "ggb_finish_general": (_I, [_I, C.POINTER(ggb_partial), C.POINTER(ggb_result)]),

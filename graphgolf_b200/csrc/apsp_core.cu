@@ -96,6 +96,10 @@ struct State {
   unsigned long long* d_ball_cnt = nullptr; size_t cap_ball_cnt = 0;
   int ball_mode = -1;         // -1 automatic, 0 never, 1 whenever feasible
   int ball_occ = 0;           // co-resident ball CTAs per SM at the last size
+  // optional per-kernel timing (ggb_set_timing): events around the two kernels
+  bool timing = false;
+  cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};   // before ball, between, after persistent
+  bool ev_ball = false;                              // the last launch ran the ball pre-pass
   long long* d_trace = nullptr;   // optional barrier trace (ggb_trace_enable)
   int trace_cap = 0;
   int trace_len = 0;
@@ -322,6 +326,7 @@ int launch_apsp(const int* d_adj, int N, int d, int n_src1, int split, int ac, i
   a.ball = use_ball ? g.d_ball : nullptr;
   a.ball_cnt = use_ball ? g.d_ball_cnt : nullptr;
   CUDA_TRY(cudaMemsetAsync(g.d_ctrl, 0, sizeof(ApspCtrl), st));
+  if (g.timing) CUDA_TRY(cudaEventRecord(g.ev[0], st));
   if (use_ball) {
     ggb::BallArgs b;
     b.adj = d_adj;
@@ -350,9 +355,12 @@ int launch_apsp(const int* d_adj, int N, int d, int n_src1, int split, int ac, i
     CUDA_TRY(cudaGetLastError());
     ++g_launches;
   }
+  if (g.timing) CUDA_TRY(cudaEventRecord(g.ev[1], st));
   void* params[] = {(void*)&a};
   CUDA_TRY(cudaLaunchCooperativeKernel(kernel_for(R), dim3(ctas), dim3(ggb::kThreads), params, smem_for(R), st));
   ++g_launches;
+  if (g.timing) CUDA_TRY(cudaEventRecord(g.ev[2], st));
+  g.ev_ball = use_ball;
   g.last_N = N;
   g.last_R = R;
   g.pending = true;
@@ -452,6 +460,8 @@ void ggb_finalize(void) {
   cudaFree(g.d_bufs);
   cudaFree(g.d_ctrl);
   cudaFree(g.d_trace);
+  for (cudaEvent_t& e : g.ev)
+    if (e) cudaEventDestroy(e);
   cudaFree(g.d_ball);
   cudaFree(g.d_ball_cnt);
   cudaFreeHost(g.h_adj);
@@ -494,6 +504,32 @@ int ggb_set_barrier_test(long long timeout_ns, int phantom) {
   if (timeout_ns <= 0 || phantom < 0) return fail(GGB_EINVAL, "timeout must be > 0, phantom >= 0");
   g.timeout_ns = timeout_ns;
   g.phantom = phantom;
+  return GGB_OK;
+}
+
+// Per-kernel timing with CUDA events recorded on the launching stream around
+// the ball pre-pass and the persistent kernel of every following launch.
+int ggb_set_timing(int enable) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  int rc = ensure_ready(-1);
+  if (rc) return rc;
+  if (enable && !g.ev[0])
+    for (cudaEvent_t& e : g.ev) CUDA_TRY(cudaEventCreate(&e));
+  g.timing = enable != 0;
+  return GGB_OK;
+}
+
+// Milliseconds of the last launch's ball pre-pass (0 if it had none) and of
+// its persistent kernel.  Waits for the launch to finish.
+int ggb_kernel_times(double* ms_ball, double* ms_persistent) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (!g.timing || !g.ev[0]) return fail(GGB_EINVAL, "timing is not enabled");
+  CUDA_TRY(cudaEventSynchronize(g.ev[2]));
+  float a = 0.f, b = 0.f;
+  CUDA_TRY(cudaEventElapsedTime(&a, g.ev[0], g.ev[1]));
+  CUDA_TRY(cudaEventElapsedTime(&b, g.ev[1], g.ev[2]));
+  if (ms_ball) *ms_ball = g.ev_ball ? a : 0.0;
+  if (ms_persistent) *ms_persistent = b;
   return GGB_OK;
 }
 

@@ -120,6 +120,20 @@ int ggb_trace_enable(int capacity);
  * returns the number of pairs copied. */
 int ggb_trace_read(long long *out, int max_pairs);
 
+/* Per-kernel timing: with enable != 0, CUDA events are recorded on the
+ * launching stream around the ball pre-pass and the persistent kernel of
+ * every following evaluation; ggb_kernel_times returns the last one's
+ * milliseconds (ball 0 when it did not run).  No counterpart in the
+ * reference; bench.py's roofline uses it. */
+int ggb_set_timing(int enable);
+int ggb_kernel_times(double *ms_ball, double *ms_persistent);
+
+/* The roof the dense sweeps run against: gathered GB/s of random-row OR
+ * sweeps (d random neighbours per row, rows of window_bits/8 bytes, N rows),
+ * one launch per sweep, on the current device with its own buffers.  No
+ * counterpart in the reference; a measurement utility for the roofline. */
+int ggb_probe_l2_gather(int N, int d, int window_bits, int iters, double *gbs);
+
 /* ---- host-buffer entry points (copy in, evaluate, copy out) ------------ */
 
 /* General graph: replaces evaluation() of general/evaluation.c:375-391 with
