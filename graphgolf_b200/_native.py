@@ -64,6 +64,8 @@ CORE_SIGNATURES = {
     "ggb_set_barrier_test": (_I, [_LL, _I]),
     "ggb_eval_general": (_I, [_I, _I, _I, _I, _P, _I, C.POINTER(ggb_result)]),
     "ggb_eval_grid": (_I, [_I, _I, _I, _P, _I, _P, C.POINTER(ggb_result)]),
+    "ggb_eval_general_nonregular": (_I, [_I, _I, _I, _I, _P, _P, _I, C.POINTER(ggb_result)]),
+    "ggb_eval_grid_nonregular": (_I, [_I, _I, _P, _I, _P, _I, _P, C.POINTER(ggb_result)]),
     "ggb_eval_general_device": (_I, [_I, _I, _I, _I, _P, _I, _P, C.POINTER(ggb_result)]),
     "ggb_launch_general_device": (_I, [_I, _I, _I, _I, _P, _I, _P]),
     "ggb_collect": (_I, [_P, C.POINTER(ggb_result)]),
@@ -99,6 +101,8 @@ LIB_FILES = {
     "core": "libgraphgolf_b200.so",
     "general": "libgg_general.so",
     "grid": "libgg_grid.so",
+    "general_nr": "libgg_general_nr.so",
+    "grid_nr": "libgg_grid_nr.so",
     "host": "libggb_host.so",
 }
 

@@ -5,7 +5,9 @@ Outputs (all under graphgolf_b200/_lib/, git-ignored, shipped with the tree):
 * ``libgraphgolf_b200.so`` -- the core: CUDA kernels for sm_100a and the
   ``ggb_*`` C ABI (include/graphgolf_b200.h).
 * ``libgg_general.so`` / ``libgg_grid.so`` -- drop-in replacements for the
-  reference's general and grid ``evaluation()`` (link-compatible C ABI).
+  reference's general and grid ``evaluation()`` (link-compatible C ABI);
+  ``libgg_general_nr.so`` / ``libgg_grid_nr.so`` the same for its
+  non-regular variants.
 * ``libggb_host.so`` -- host C utilities: seeded generators, edge files,
   adjacency, checks.
 
@@ -76,7 +78,8 @@ def build(verbose: bool = False) -> dict[str, Path]:
             Path(o).unlink(missing_ok=True)
     out["core"] = core
 
-    for name, src in (("general", "dropin_general.c"), ("grid", "dropin_grid.c")):
+    for name, src in (("general", "dropin_general.c"), ("grid", "dropin_grid.c"),
+                      ("general_nr", "dropin_general_nonregular.c"), ("grid_nr", "dropin_grid_nonregular.c")):
         so = LIB / f"libgg_{name}.so"
         deps = [CSRC / src, INCLUDE / "graphgolf_b200.h", core]
         if _stale(so, deps):

@@ -31,15 +31,20 @@ namespace ggb {
 // relabelled adjacency holds rotate_hash[adj[i][j]].  inv[] must be -1 on
 // entry; it receives the inverse permutation so a second kernel can verify
 // that rotate_hash is a bijection.
+// With deg (non-regular grids, degree[i] entries of row i are edges), the
+// slots j >= deg[i] are filled with the row's own relabelled id: OR-ing a
+// row's own set into itself changes nothing, so the sweep needs no per-row
+// degree.
 __global__ void relabel_adjacency_kernel(const int* __restrict__ adj, const int* __restrict__ rh,
                                          int* __restrict__ out, int* __restrict__ inv, int N, int d,
-                                         ApspCtrl* ctrl) {
+                                         ApspCtrl* ctrl, const int* __restrict__ deg) {
   const long long n = (long long)N * d;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
        e += (long long)gridDim.x * blockDim.x) {
     const int i = (int)(e / d), j = (int)(e % d);
     const int r = rh[i];
-    const int nb = adj[e];
+    if (deg && ((unsigned)deg[i] > (unsigned)d)) { set_error(ctrl, kErrDegree, i); continue; }
+    const int nb = (deg && j >= deg[i]) ? i : adj[e];
     if ((unsigned)r >= (unsigned)N) { set_error(ctrl, kErrPerm, i); continue; }
     if ((unsigned)nb >= (unsigned)N) { set_error(ctrl, kErrAdj, i); continue; }
     const int rn = rh[nb];
@@ -54,6 +59,20 @@ __global__ void relabel_adjacency_kernel(const int* __restrict__ adj, const int*
       if ((unsigned)r >= (unsigned)N) { set_error(ctrl, kErrPerm, (int)i); continue; }
       inv[r] = (int)i;
     }
+  }
+}
+
+// Non-regular general graphs: out[i][j] = adj[i][j] for j < deg[i], else i
+// (a self entry, which the recurrence ignores).
+__global__ void pad_adjacency_kernel(const int* __restrict__ adj, const int* __restrict__ deg,
+                                     int* __restrict__ out, int N, int d, ApspCtrl* ctrl) {
+  const long long n = (long long)N * d;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(e / d), j = (int)(e % d);
+    const int di = deg[i];
+    if ((unsigned)di > (unsigned)d) { set_error(ctrl, kErrDegree, i); continue; }
+    out[e] = j < di ? adj[e] : i;
   }
 }
 
@@ -81,6 +100,8 @@ struct State {
   int* d_adj2 = nullptr;      size_t cap_adj2 = 0;    // ints (grid relabel)
   int* d_rh = nullptr;        size_t cap_rh = 0;      // ints
   int* d_inv = nullptr;       size_t cap_inv = 0;     // ints
+  int* d_deg = nullptr;       size_t cap_deg = 0;     // ints (non-regular degrees)
+  int* h_deg = nullptr;       size_t cap_hdeg = 0;
   uint4* d_bufs = nullptr;    size_t cap_buf = 0;     // uint4, both bitset matrices
   ApspCtrl* d_ctrl = nullptr;
   // pinned host staging
@@ -263,7 +284,7 @@ int choose_R(int N, int d, int nsrc_max) {
 }
 
 int launch_apsp(const int* d_adj, int N, int d, int n_src1, int split, int ac, int groups,
-                int rank, int procs, cudaStream_t st) {
+                int rank, int procs, cudaStream_t st, const int* d_adj2 = nullptr) {
   const int R = choose_R(N, d, std::max(n_src1, ac));
   const int ri = r_index(R);
   if (ri < 0) return fail(GGB_EINVAL, "window of %d uint4 per row is not supported", R);
@@ -307,6 +328,7 @@ int launch_apsp(const int* d_adj, int N, int d, int n_src1, int split, int ac, i
 
   ApspArgs a;
   a.adj = d_adj;
+  a.adj2 = d_adj2;
   a.buf0 = g.d_bufs;
   a.buf1 = g.d_bufs + cells;
   a.ctrl = g.d_ctrl;
@@ -378,6 +400,8 @@ int read_ctrl(cudaStream_t st, ggb_partial* p) {
     return fail(GGB_EPERM, "rotate_hash is not a permutation of [0, nodes) (at %d)", c.error_info);
   if (c.error == ggb::kErrTimeout)
     return fail(GGB_ETIMEOUT, "a grid-barrier wait ran out (CTA %d)", c.error_info);
+  if (c.error == ggb::kErrDegree)
+    return fail(GGB_EINVAL, "degree of vertex %d outside [0, max_degree]", c.error_info);
   if (c.error != 0) return fail(GGB_ECUDA, "device error code %d", c.error);
   if (!c.done) return fail(GGB_ECUDA, "the persistent kernel did not complete");
   p->diam = c.diam;
@@ -415,6 +439,16 @@ int stage_adj(const int* adj, size_t n, cudaStream_t st) {
     std::memcpy(g.h_adj, adj, n * sizeof(int));
     CUDA_TRY(cudaMemcpyAsync(g.d_adj, g.h_adj, n * sizeof(int), cudaMemcpyHostToDevice, st));
   }
+  return GGB_OK;
+}
+
+int stage_deg(const int* deg, size_t n, cudaStream_t st) {
+  int rc = grow_device(&g.d_deg, &g.cap_deg, n);
+  if (rc) return rc;
+  rc = grow_pinned(&g.h_deg, &g.cap_hdeg, n);
+  if (rc) return rc;
+  std::memcpy(g.h_deg, deg, n * sizeof(int));
+  CUDA_TRY(cudaMemcpyAsync(g.d_deg, g.h_deg, n * sizeof(int), cudaMemcpyHostToDevice, st));
   return GGB_OK;
 }
 
@@ -457,6 +491,8 @@ void ggb_finalize(void) {
   cudaFree(g.d_adj2);
   cudaFree(g.d_rh);
   cudaFree(g.d_inv);
+  cudaFree(g.d_deg);
+  cudaFreeHost(g.h_deg);
   cudaFree(g.d_bufs);
   cudaFree(g.d_ctrl);
   cudaFree(g.d_trace);
@@ -658,8 +694,15 @@ int ggb_eval_general_device(int nodes, int based_nodes, int groups, int degree, 
   return ggb_collect(stream, out);
 }
 
-int ggb_eval_grid(int nodes, int degree, int groups, const int* adj, int based_nodes,
-                  const int* rotate_hash, ggb_result* out) {
+}  // extern "C"
+
+namespace {
+
+// Grid evaluation, regular (deg == nullptr) or not: relabel by rotate_hash
+// on the device (padding the rows of a non-regular grid with their own id),
+// check the relabel is a bijection, then run the persistent kernel.
+int eval_grid_impl(int nodes, int degree, const int* deg, int groups, const int* adj, int based_nodes,
+                   const int* rotate_hash, ggb_result* out) {
   std::lock_guard<std::mutex> lk(g_mu);
   if (!out || !rotate_hash || (!adj && nodes * degree)) return fail(GGB_EINVAL, "null pointer");
   if (nodes <= 0 || based_nodes <= 0 || groups <= 0 || degree < 0 || based_nodes > nodes)
@@ -675,6 +718,7 @@ int ggb_eval_grid(int nodes, int degree, int groups, const int* adj, int based_n
   if ((rc = grow_device(&g.d_rh, &g.cap_rh, (size_t)nodes))) return rc;
   if ((rc = grow_device(&g.d_inv, &g.cap_inv, (size_t)nodes))) return rc;
   if ((rc = grow_pinned(&g.h_rh, &g.cap_hrh, (size_t)nodes))) return rc;
+  if (deg && (rc = stage_deg(deg, (size_t)nodes, st))) return rc;
   std::memcpy(g.h_rh, rotate_hash, (size_t)nodes * sizeof(int));
   CUDA_TRY(cudaMemcpyAsync(g.d_rh, g.h_rh, (size_t)nodes * sizeof(int), cudaMemcpyHostToDevice, st));
   CUDA_TRY(cudaMemsetAsync(g.d_ctrl, 0, sizeof(ApspCtrl), st));
@@ -683,7 +727,7 @@ int ggb_eval_grid(int nodes, int degree, int groups, const int* adj, int based_n
   const long long work = std::max<long long>((long long)n, nodes);
   const int blocks = (int)std::min<long long>((work + threads - 1) / threads, (long long)g.sms * 8);
   ggb::relabel_adjacency_kernel<<<blocks, threads, 0, st>>>(g.d_adj, g.d_rh, g.d_adj2, g.d_inv, nodes, degree,
-                                                            g.d_ctrl);
+                                                            g.d_ctrl, deg ? g.d_deg : nullptr);
   CUDA_TRY(cudaGetLastError());
   ggb::check_permutation_kernel<<<std::min(blocks, g.sms * 4), threads, 0, st>>>(g.d_inv, nodes, g.d_ctrl);
   CUDA_TRY(cudaGetLastError());
@@ -692,6 +736,8 @@ int ggb_eval_grid(int nodes, int degree, int groups, const int* adj, int based_n
   CUDA_TRY(cudaStreamSynchronize(st));
   if (g.h_ctrl->error == ggb::kErrAdj)
     return fail(GGB_EADJ, "adjacency entry outside [0, nodes) (row %d)", g.h_ctrl->error_info);
+  if (g.h_ctrl->error == ggb::kErrDegree)
+    return fail(GGB_EINVAL, "degree[%d] outside [0, max_degree]", g.h_ctrl->error_info);
   if (g.h_ctrl->error != 0)
     return fail(GGB_EPERM, "rotate_hash is not a permutation of [0, nodes) (at %d)", g.h_ctrl->error_info);
   g.last_grid = true;
@@ -701,6 +747,57 @@ int ggb_eval_grid(int nodes, int degree, int groups, const int* adj, int based_n
   rc = read_ctrl(st, &p);
   if (rc) return rc;
   return ggb_finish_grid(nodes, &p, out);
+}
+
+}  // namespace
+
+extern "C" {
+
+int ggb_eval_grid(int nodes, int degree, int groups, const int* adj, int based_nodes,
+                  const int* rotate_hash, ggb_result* out) {
+  return eval_grid_impl(nodes, degree, nullptr, groups, adj, based_nodes, rotate_hash, out);
+}
+
+int ggb_eval_grid_nonregular(int nodes, int max_degree, const int* degree, int groups, const int* adj,
+                             int based_nodes, const int* rotate_hash, ggb_result* out) {
+  if (!degree) return fail(GGB_EINVAL, "null degree array");
+  return eval_grid_impl(nodes, max_degree, degree, groups, adj, based_nodes, rotate_hash, out);
+}
+
+int ggb_eval_general_nonregular(int nodes, int based_nodes, int groups, int max_degree, const int* num_degrees,
+                                const int* adj, int added_centers, ggb_result* out) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (!out || !num_degrees || (!adj && nodes * max_degree)) return fail(GGB_EINVAL, "null pointer");
+  int rc = check_general(nodes, based_nodes, groups, max_degree, added_centers);
+  if (rc) return rc;
+  rc = ensure_ready(-1);
+  if (rc) return rc;
+  const size_t n = (size_t)nodes * max_degree;
+  cudaStream_t st = g.stream;
+  rc = stage_adj(adj, n, st);
+  if (rc) return rc;
+  if ((rc = grow_device(&g.d_adj2, &g.cap_adj2, n))) return rc;
+  if ((rc = stage_deg(num_degrees, (size_t)nodes, st))) return rc;
+  CUDA_TRY(cudaMemsetAsync(g.d_ctrl, 0, sizeof(ApspCtrl), st));
+  const int threads = 256;
+  const int blocks = (int)std::min<long long>(((long long)n + threads - 1) / threads + 1, (long long)g.sms * 8);
+  ggb::pad_adjacency_kernel<<<blocks, threads, 0, st>>>(g.d_adj, g.d_deg, g.d_adj2, nodes, max_degree, g.d_ctrl);
+  CUDA_TRY(cudaGetLastError());
+  ++g_launches;
+  CUDA_TRY(cudaMemcpyAsync(g.h_ctrl, g.d_ctrl, sizeof(ApspCtrl), cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  if (g.h_ctrl->error != 0)
+    return fail(GGB_EINVAL, "num_degrees[%d] outside [0, max_degree]", g.h_ctrl->error_info);
+  g.last_grid = false;
+  // phase 1 gathers the padded rows; the added-centre phase gathers whole rows
+  // (variants/not_regular_general_graph/evaluation.c:180 vs :226)
+  rc = launch_apsp(g.d_adj2, nodes, max_degree, based_nodes, based_nodes * groups, added_centers, groups, 0, 1, st,
+                   added_centers ? g.d_adj : nullptr);
+  if (rc) return rc;
+  ggb_partial p;
+  rc = read_ctrl(st, &p);
+  if (rc) return rc;
+  return ggb_finish_general(nodes, &p, out);
 }
 
 }  // extern "C"

@@ -49,7 +49,7 @@ constexpr int kBallMaxWindows = 32;   // windows of one rank in the ball pre-pas
 constexpr int kBallMaxDegree = 32;
 
 // Error codes written to ApspCtrl::error (host maps them to GGB_E*).
-enum : int { kErrNone = 0, kErrAdj = 1, kErrTimeout = 2, kErrPerm = 3 };
+enum : int { kErrNone = 0, kErrAdj = 1, kErrTimeout = 2, kErrPerm = 3, kErrDegree = 4 };
 
 // Device-side control block.  Zeroed by the host before every launch.
 struct ApspCtrl {
@@ -70,6 +70,8 @@ struct ApspCtrl {
 
 struct ApspArgs {
   const int* adj;        // [N][d], device, rows already relabelled (grid)
+  const int* adj2;       // rows the added-centre phase gathers, or null for adj; the non-regular
+                         // evaluators gather padded rows in phase 1 but whole rows here
   uint4* buf0;           // [N][R]
   uint4* buf1;           // [N][R]
   ApspCtrl* ctrl;
@@ -384,7 +386,8 @@ constexpr int kSeedNb = 64;                      // neighbour ids staged per ver
 // out coalesced.  Replaces the reference's clear + identity set-up (:168-172)
 // and its first two OR-gather sweeps.
 template <int R, int VEC>
-__device__ __forceinline__ void seed_window(const ApspArgs& a, int base, int l, uint4* s2_out, int* s_nb,
+__device__ __forceinline__ void seed_window(const ApspArgs& a, const int* __restrict__ adj, int base, int l,
+                                            uint4* s2_out, int* s_nb,
                                             unsigned* s_rw, unsigned (&c)[4], bool& adj_ok, long long warp_id,
                                             long long n_warps) {
   constexpr int SROW = 4 * R;
@@ -404,7 +407,7 @@ __device__ __forceinline__ void seed_window(const ApspArgs& a, int base, int l, 
       const int dc = min(kSeedNb, d - jb);
       __syncwarp();
       if (live)
-        for (int j = r; j < dc; j += kSeedGroup) nb[j] = __ldg(a.adj + v * d + jb + j);
+        for (int j = r; j < dc; j += kSeedGroup) nb[j] = __ldg(adj + v * d + jb + j);
       __syncwarp();
       if (!live) continue;
       for (int j = r; j < dc; j += kSeedGroup) {
@@ -412,7 +415,7 @@ __device__ __forceinline__ void seed_window(const ApspArgs& a, int base, int l, 
         if ((unsigned)x >= (unsigned)N) { adj_ok = false; continue; }
         set_bit_in(s1, x, base, l);
       }
-      set_rows_bits<VEC, kSeedGroup>(a.adj, N, d, nb, dc, s2, base, l, r, adj_ok, nullptr);
+      set_rows_bits<VEC, kSeedGroup>(adj, N, d, nb, dc, s2, base, l, r, adj_ok, nullptr);
     }
     __syncwarp();
 #pragma unroll
@@ -679,6 +682,7 @@ __global__ void __launch_bounds__(kThreads, 1) apsp_persistent_kernel(const Apsp
     const int row0 = phase == 1 ? 0 : N - a.ac;
     const int nwin = (nsrc + W - 1) / W;
     const bool use_ball = phase == 1 && a.ball != nullptr;
+    const int* __restrict__ adjp = (phase == 2 && a.adj2) ? a.adj2 : a.adj;
     int local = 0;
     for (int t = a.win_first; t < nwin && !disconnected; t += a.win_stride, ++local) {
       const int first = t * W;
@@ -710,9 +714,9 @@ __global__ void __launch_bounds__(kThreads, 1) apsp_persistent_kernel(const Apsp
         // ---- levels 0 and 1 by two-hop seeding into buf0 -----------------------
         unsigned c[4] = {0u, 0u, 0u, 0u};  // S_1 lo, S_1 hi, S_2 lo, S_2 hi
         if (a.vec4)
-          seed_window<R, 4>(a, base, l, a.buf0, my_nb, my_rows, c, adj_ok, warp_id, n_warps);
+          seed_window<R, 4>(a, adjp, base, l, a.buf0, my_nb, my_rows, c, adj_ok, warp_id, n_warps);
         else
-          seed_window<R, 1>(a, base, l, a.buf0, my_nb, my_rows, c, adj_ok, warp_id, n_warps);
+          seed_window<R, 1>(a, adjp, base, l, a.buf0, my_nb, my_rows, c, adj_ok, warp_id, n_warps);
         if (!adj_ok) set_error(a.ctrl, kErrAdj, (int)blockIdx.x);
         cta_add_counts<4>(c, a.ctrl, gl, s_red);
         bar_target += grid;
@@ -748,11 +752,11 @@ __global__ void __launch_bounds__(kThreads, 1) apsp_persistent_kernel(const Apsp
           if constexpr (LPR == 32) {
             if (d <= 32 && !own_count && prev_total * 10 >= (long long)N * l * 9) {
               wide = true;
-              sweep_wide<R>(src, dst, a.adj, N, d, a.split, slot, n_slots, l, own_count, cl, adj_ok);
+              sweep_wide<R>(src, dst, adjp, N, d, a.split, slot, n_slots, l, own_count, cl, adj_ok);
             }
           }
           for (long long v = wide ? N : slot; v < N; v += n_slots) {
-            const int* arow = a.adj + v * d;
+            const int* arow = adjp + v * d;
             uint4 acc[UPL];
 #pragma unroll
             for (int k = 0; k < UPL; ++k) acc[k] = ld_cg(src + v * R + li + k * LPR);

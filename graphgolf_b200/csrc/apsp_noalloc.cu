@@ -154,6 +154,7 @@ extern "C" int ggb_eval_general_noalloc(int nodes, int based_nodes, int groups, 
 
   ggb::ApspArgs a;
   a.adj = adj_dev;
+  a.adj2 = nullptr;
   a.buf0 = bufs;
   a.buf1 = bufs + cells;
   a.ctrl = ctrl;

@@ -86,6 +86,41 @@ def evaluate_grid(adj, rotate_hash, groups: int = 1, based_nodes: int | None = N
     return Result.from_c(r)
 
 
+def evaluate_nonregular(adj, num_degrees, based_nodes: int | None = None, groups: int = 1,
+                        added_centers: int = 0) -> Result:
+    """Exact APSP of a non-regular general graph: row i of the
+    [nodes][max_degree] adjacency holds num_degrees[i] neighbours
+    (variants/not_regular_general_graph/evaluation.c:378-393)."""
+    a = np.ascontiguousarray(adj, dtype=np.int32)
+    nodes, max_degree = a.shape
+    nd = np.ascontiguousarray(num_degrees, dtype=np.int32)
+    if nd.shape != (nodes,):
+        raise EvaluationError(-1, "num_degrees must have one entry per vertex")
+    if based_nodes is None:
+        based_nodes = (nodes - added_centers) // groups
+    r = ggb_result()
+    _raise(load().ggb_eval_general_nonregular(nodes, based_nodes, groups, max_degree, nd.ctypes.data,
+                                              a.ctypes.data, added_centers, C.byref(r)))
+    return Result.from_c(r)
+
+
+def evaluate_grid_nonregular(adj, degree, rotate_hash, groups: int = 1, based_nodes: int | None = None) -> Result:
+    """Exact APSP of a non-regular grid graph (variants/not_regular_grid_graph/
+    evaluation.c:192-207): row i holds degree[i] neighbours."""
+    a = np.ascontiguousarray(adj, dtype=np.int32)
+    nodes, max_degree = a.shape
+    dg = np.ascontiguousarray(degree, dtype=np.int32)
+    rh = np.ascontiguousarray(rotate_hash, dtype=np.int32)
+    if dg.shape != (nodes,) or rh.shape != (nodes,):
+        raise EvaluationError(-1, "degree and rotate_hash must have one entry per vertex")
+    if based_nodes is None:
+        based_nodes = nodes // groups
+    r = ggb_result()
+    _raise(load().ggb_eval_grid_nonregular(nodes, max_degree, dg.ctypes.data, groups, a.ctypes.data, based_nodes,
+                                           rh.ctypes.data, C.byref(r)))
+    return Result.from_c(r)
+
+
 def evaluation(nodes: int, based_nodes: int, groups: int, lines: int, degree: int, adj,
                added_centers: int = 0, algo: int = MATRIX_OP) -> tuple[bool, int, float]:
     """general evaluation(): returns (connected, diameter, ASPL) as the C

@@ -133,3 +133,25 @@ def verify(g: Graph, max_len: int = 0) -> int:
     """0 if regular, loop-free, duplicate-free (and length-bounded); else 1..4."""
     e = np.ascontiguousarray(g.edges, dtype=np.int32)
     return int(load("host").ggbh_verify(g.nodes, e.shape[0], g.degree, _ptr(e), max_len, g.height))
+
+
+def nonregular(g: Graph, drop: int, seed: int, pad: int = -1) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+    """Removes `drop` seeded random edges from g and returns (edges, adj,
+    degrees): adj is [nodes][g.degree] with each row's neighbours first in
+    edge order (as the non-regular programs' create_adj) and `pad` in the
+    unused slots (pad < 0 means the row's own id, a valid vertex)."""
+    rng = np.random.default_rng(seed)
+    keep = np.ones(g.lines, dtype=bool)
+    keep[rng.choice(g.lines, size=drop, replace=False)] = False
+    edges = np.ascontiguousarray(g.edges[keep], dtype=np.int32)
+    n, d = g.nodes, g.degree
+    adj = np.empty((n, d), dtype=np.int32)
+    adj[:] = np.arange(n, dtype=np.int32)[:, None] if pad < 0 else pad
+    deg = np.zeros(n, dtype=np.int32)
+    for a, b in edges:
+        adj[a, deg[a]] = b
+        deg[a] += 1
+        adj[b, deg[b]] = a
+        deg[b] += 1
+    return edges, adj, deg
+

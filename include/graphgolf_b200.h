@@ -152,6 +152,22 @@ int ggb_eval_general(int nodes, int based_nodes, int groups, int degree, const i
 int ggb_eval_grid(int nodes, int degree, int groups, const int *adj, int based_nodes,
                   const int *rotate_hash, ggb_result *out);
 
+/* Non-regular general graph: replaces evaluation() of
+ * variants/not_regular_general_graph/evaluation.c:378-393.  Row i of the
+ * [nodes][max_degree] adjacency holds num_degrees[i] neighbours; the BFS over
+ * the based sources reads only those (:180), the added-centre phase reads the
+ * whole row, padding included, as the reference does (:226).  Same return
+ * convention as ggb_eval_general; num_degrees[i] outside [0, max_degree] is
+ * rejected with GGB_EINVAL. */
+int ggb_eval_general_nonregular(int nodes, int based_nodes, int groups, int max_degree, const int *num_degrees,
+                                const int *adj, int added_centers, ggb_result *out);
+
+/* Non-regular grid graph: replaces evaluation() of
+ * variants/not_regular_grid_graph/evaluation.c:192-207 (matrix path); row i
+ * holds degree[i] neighbours (:149-151).  Grid return convention. */
+int ggb_eval_grid_nonregular(int nodes, int max_degree, const int *degree, int groups, const int *adj,
+                             int based_nodes, const int *rotate_hash, ggb_result *out);
+
 /* ---- device-resident entry points (inputs already in HBM) -------------- */
 
 /* Same as ggb_eval_general with adj_dev a device pointer.  Enqueues on

@@ -55,12 +55,18 @@ def port() -> C.CDLL:
         lib.oracle_grid_partial.argtypes = [I, I, I, P, I, P, I, I, IP, LP]
         lib.oracle_grid_finish.argtypes = [I, I, LL, IP, DP]
         lib.oracle_bfs_sums.argtypes = [I, I, P, P, I, IP, LP]
+        lib.oracle_general_eval_nr.argtypes = [I, I, I, I, P, P, I, I, IP, DP, LP]
+        lib.oracle_grid_eval_nr.argtypes = [I, I, P, I, P, I, P, IP, DP, LP]
         _port = lib
     return _port
 
 
 def have_ref() -> bool:
     return (REF_DIR / "libref_general.so").exists() and (REF_DIR / "libref_grid.so").exists()
+
+
+def have_ref_nr() -> bool:
+    return (REF_DIR / "libref_general_nr.so").exists() and (REF_DIR / "libref_grid_nr.so").exists()
 
 
 def _ref(kind: str) -> C.CDLL:
@@ -171,3 +177,81 @@ def ref_grid(adj, rotate_hash, groups=1, based_nodes=None, height=0, based_heigh
     ok = lib.evaluation(n, d, groups, a.ctypes.data, based_nodes, height, based_height, C.byref(dm),
                         C.byref(asp), bool(enable_bfs), rh.ctypes.data)
     return bool(ok), dm.value, (asp.value if ok else None)
+
+
+def general_nr(adj, degs, based_nodes=None, groups=1, added_centers=0, algo=1):
+    """Port, non-regular general: returns (connected, diameter, aspl, total)."""
+    a = _adj(adj)
+    n, d = a.shape
+    nd = np.ascontiguousarray(degs, dtype=np.int32)
+    if based_nodes is None:
+        based_nodes = (n - added_centers) // groups
+    dm, asp, tot = C.c_int(0), C.c_double(0.0), C.c_longlong(0)
+    rc = port().oracle_general_eval_nr(n, based_nodes, groups, d, nd.ctypes.data, a.ctypes.data, added_centers,
+                                       algo, C.byref(dm), C.byref(asp), C.byref(tot))
+    if rc < 0:
+        raise ValueError(f"oracle_general_eval_nr: {rc}")
+    return bool(rc), dm.value, asp.value, (tot.value if rc else 0)
+
+
+def grid_nr(adj, degs, rotate_hash, groups=1, based_nodes=None):
+    """Port, non-regular grid: returns (connected, diameter, aspl or None, total)."""
+    a = _adj(adj)
+    n, d = a.shape
+    nd = np.ascontiguousarray(degs, dtype=np.int32)
+    rh = np.ascontiguousarray(rotate_hash, dtype=np.int32)
+    if based_nodes is None:
+        based_nodes = n // groups
+    dm, asp, tot = C.c_int(0), C.c_double(float("nan")), C.c_longlong(0)
+    rc = port().oracle_grid_eval_nr(n, d, nd.ctypes.data, groups, a.ctypes.data, based_nodes, rh.ctypes.data,
+                                    C.byref(dm), C.byref(asp), C.byref(tot))
+    if rc < 0:
+        raise ValueError(f"oracle_grid_eval_nr: {rc}")
+    return bool(rc), dm.value, (asp.value if rc else None), (tot.value if rc else 0)
+
+
+_ref_nr = {}
+
+
+def ref_general_nr(adj, degs, based_nodes=None, groups=1, added_centers=0, algo=1):
+    """The reference's non-regular general evaluation(): (connected, diameter, aspl)."""
+    if "g" not in _ref_nr:
+        lib = C.CDLL(str(REF_DIR / "libref_general_nr.so"))
+        lib.evaluation.restype = C.c_bool
+        lib.evaluation.argtypes = [C.c_int] * 5 + [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_double), C.c_int,
+                                                   C.c_void_p, C.c_int]
+        lib.ref_set_ranks(0, 1)
+        _ref_nr["g"] = lib
+    lib = _ref_nr["g"]
+    a = _adj(adj)
+    n, d = a.shape
+    nd = np.ascontiguousarray(degs, dtype=np.int32)
+    if based_nodes is None:
+        based_nodes = (n - added_centers) // groups
+    dm, asp = C.c_int(0), C.c_double(0.0)
+    ok = lib.evaluation(n, based_nodes, groups, int(nd.sum()) // 2, d, a.ctypes.data, C.byref(dm), C.byref(asp),
+                        added_centers, nd.ctypes.data, algo)
+    return bool(ok), dm.value, asp.value
+
+
+def ref_grid_nr(adj, degs, rotate_hash, groups=1, based_nodes=None):
+    """The reference's non-regular grid evaluation(): (connected, diameter, aspl or None)."""
+    if "r" not in _ref_nr:
+        lib = C.CDLL(str(REF_DIR / "libref_grid_nr.so"))
+        lib.evaluation.restype = C.c_bool
+        lib.evaluation.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int,
+                                   C.POINTER(C.c_int), C.POINTER(C.c_double), C.c_bool, C.c_void_p]
+        lib.ref_set_ranks(0, 1)
+        _ref_nr["r"] = lib
+    lib = _ref_nr["r"]
+    a = _adj(adj)
+    n, d = a.shape
+    nd = np.ascontiguousarray(degs, dtype=np.int32)
+    rh = np.ascontiguousarray(rotate_hash, dtype=np.int32)
+    if based_nodes is None:
+        based_nodes = n // groups
+    dm, asp = C.c_int(0), C.c_double(float("nan"))
+    ok = lib.evaluation(n, d, nd.ctypes.data, groups, a.ctypes.data, based_nodes, 0, 0, C.byref(dm), C.byref(asp),
+                        False, rh.ctypes.data)
+    return bool(ok), dm.value, (asp.value if ok else None)
+

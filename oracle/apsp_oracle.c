@@ -10,6 +10,8 @@
  *   - general/evaluation.c:265-373  matrix_op_mem_saving (4096-source passes, CHUNK=64 words)
  *   - general/evaluation.c:375-391  evaluation()          (dispatch, return convention)
  *   - grid/evaluation.c:122-190     matrix_op            (rotate_hash relabel, grid return convention)
+ *   - variants/not_regular_general_graph/evaluation.c:156-393, variants/not_regular_grid_graph/
+ *     evaluation.c:122-207: the same loops with a per-row neighbour count
  * and, as an independent second check, a plain queue BFS
  *   - general/evaluation.c:55-150   bfs (ASPL over half the matrix with symmetry weights)
  *
@@ -37,6 +39,8 @@ typedef struct {
   int degree;
   const int *adj;      /* [nodes][degree]                                  */
   const int *relabel;  /* grid rotate_hash, or NULL for the identity       */
+  const int *degs;     /* per-row neighbour counts (non-regular variants), or
+                          NULL: every row has `degree` neighbours            */
 } oracle_graph;
 
 /* Per-level accounting of one source window: which rows the termination test
@@ -76,7 +80,10 @@ static long long run_window(const oracle_graph *g, uint64_t *A, uint64_t *B, int
     for (int i = 0; i < n; i++) {
       int row = g->relabel ? g->relabel[i] : i;
       uint64_t *dst = B + (size_t)row * w;
-      for (int j = 0; j < d; j++) {
+      /* non-regular variants: only the row's first degs[i] entries are edges
+         (variants/not_regular_general_graph/evaluation.c:180, not_regular_grid_graph :149) */
+      const int dj = g->degs ? g->degs[i] : d;
+      for (int j = 0; j < dj; j++) {
         int nb = g->adj[(size_t)i * d + j];
         int src_row = g->relabel ? g->relabel[nb] : nb;
         const uint64_t *src = A + (size_t)src_row * w;
@@ -107,9 +114,9 @@ static long long run_window(const oracle_graph *g, uint64_t *A, uint64_t *B, int
  * value a fixed width as MATRIX_OP_MEM_SAVING does with CHUNK=64 (:269-273).
  * Returns 0, or a negative error for invalid arguments / no memory.
  */
-int oracle_general_partial(int nodes, int based_nodes, int groups, int degree, const int *adj,
-                           int added_centers, int words_per_row, int rank, int procs,
-                           int *diam_partial, long long *sum_partial)
+static int general_partial_impl(int nodes, int based_nodes, int groups, int degree, const int *adj,
+                                const int *degs, int added_centers, int words_per_row, int rank, int procs,
+                                int *diam_partial, long long *sum_partial)
 {
   if (nodes <= 0 || based_nodes <= 0 || groups <= 0 || degree < 0 || procs <= 0 || rank < 0 ||
       rank >= procs || added_centers < 0 || based_nodes * groups + added_centers != nodes)
@@ -128,7 +135,7 @@ int oracle_general_partial(int nodes, int based_nodes, int groups, int degree, c
   uint64_t *A = malloc(cells * sizeof(uint64_t)), *B = malloc(cells * sizeof(uint64_t));
   if (!A || !B) { free(A); free(B); return ORACLE_ENOMEM; }
 
-  oracle_graph g = {nodes, (int)chunk, degree, adj, NULL};
+  oracle_graph g = {nodes, (int)chunk, degree, adj, NULL, degs};
   long long sum = 0;
   long long diam = 1;  /* *diam = 1 (:165) */
 
@@ -149,7 +156,9 @@ int oracle_general_partial(int nodes, int based_nodes, int groups, int degree, c
     unsigned p2 = (e2 + c2 - 1) / c2;
     int s = based_nodes % procs;
     int new_rank = (rank - s >= 0) ? rank - s : rank - s + procs;
-    oracle_graph g2 = {nodes, (int)c2, degree, adj, NULL};
+    /* the non-regular variant's centre phase reads whole rows
+     * (variants/not_regular_general_graph/evaluation.c:226) */
+    oracle_graph g2 = {nodes, (int)c2, degree, adj, NULL, NULL};
     oracle_window_rule r2 = {based_nodes * groups, 1, 0, added_centers, 0, 1};
     for (unsigned t = (unsigned)new_rank; t < p2; t += procs) {
       long long first = 64LL * t * c2;
@@ -163,6 +172,14 @@ int oracle_general_partial(int nodes, int based_nodes, int groups, int degree, c
   *diam_partial = diam > INT_MAX ? INT_MAX : (int)diam;
   *sum_partial = sum;
   return ORACLE_OK;
+}
+
+int oracle_general_partial(int nodes, int based_nodes, int groups, int degree, const int *adj,
+                           int added_centers, int words_per_row, int rank, int procs,
+                           int *diam_partial, long long *sum_partial)
+{
+  return general_partial_impl(nodes, based_nodes, groups, degree, adj, NULL, added_centers, words_per_row, rank,
+                              procs, diam_partial, sum_partial);
 }
 
 /* The tail of general/evaluation.c:247-262 once the partials are reduced
@@ -196,12 +213,27 @@ int oracle_general_eval(int nodes, int based_nodes, int groups, int degree, cons
   return oracle_general_finish(nodes, dp, sp, diameter, ASPL);
 }
 
+/* variants/not_regular_general_graph/evaluation.c:156-393: the same with
+ * row i holding num_degrees[i] neighbours (max_degree slots). */
+int oracle_general_eval_nr(int nodes, int based_nodes, int groups, int max_degree, const int *num_degrees,
+                           const int *adj, int added_centers, int algo, int *diameter, double *ASPL,
+                           long long *sum_out)
+{
+  int dp;
+  long long sp;
+  int rc = general_partial_impl(nodes, based_nodes, groups, max_degree, adj, num_degrees, added_centers,
+                                algo == 2 ? 64 : 0, 0, 1, &dp, &sp);
+  if (rc) return rc;
+  if (sum_out) *sum_out = sp + (long long)nodes * (nodes - 1);
+  return oracle_general_finish(nodes, dp, sp, diameter, ASPL);
+}
+
 /* grid/evaluation.c:122-190 on one rank: the same level loop over relabelled
  * rows, sources = relabelled ids 0..based_nodes-1, weight `groups`.  The grid
  * convention differs from the general one: disconnected means diameter >
  * nodes, the diameter is still written, and ASPL is left untouched. */
-int oracle_grid_partial(int nodes, int degree, int groups, const int *adj, int based_nodes,
-                        const int *rotate_hash, int rank, int procs, int *diam_partial, long long *sum_partial)
+static int grid_partial_impl(int nodes, int degree, const int *degs, int groups, const int *adj, int based_nodes,
+                             const int *rotate_hash, int rank, int procs, int *diam_partial, long long *sum_partial)
 {
   if (nodes <= 0 || based_nodes <= 0 || groups <= 0 || degree < 0 || procs <= 0 || rank < 0 || rank >= procs)
     return ORACLE_EINVAL;
@@ -211,7 +243,7 @@ int oracle_grid_partial(int nodes, int degree, int groups, const int *adj, int b
   size_t cells = (size_t)nodes * chunk;
   uint64_t *A = malloc(cells * sizeof(uint64_t)), *B = malloc(cells * sizeof(uint64_t));
   if (!A || !B) { free(A); free(B); return ORACLE_ENOMEM; }
-  oracle_graph g = {nodes, (int)chunk, degree, adj, rotate_hash};
+  oracle_graph g = {nodes, (int)chunk, degree, adj, rotate_hash, degs};
   oracle_window_rule r = {nodes, 0, nodes, 0, groups, 0};
   long long sum = 0, diam = 1;
   for (unsigned t = (unsigned)rank; t < parsize; t += procs) {
@@ -225,6 +257,13 @@ int oracle_grid_partial(int nodes, int degree, int groups, const int *adj, int b
   *diam_partial = diam > INT_MAX ? INT_MAX : (int)diam;
   *sum_partial = sum;
   return ORACLE_OK;
+}
+
+int oracle_grid_partial(int nodes, int degree, int groups, const int *adj, int based_nodes,
+                        const int *rotate_hash, int rank, int procs, int *diam_partial, long long *sum_partial)
+{
+  return grid_partial_impl(nodes, degree, NULL, groups, adj, based_nodes, rotate_hash, rank, procs, diam_partial,
+                           sum_partial);
 }
 
 int oracle_grid_finish(int nodes, int diam, long long sum, int *diameter, double *ASPL)
@@ -289,4 +328,17 @@ int oracle_bfs_sums(int nodes, int degree, const int *adj, const int *relabel, i
   *ecc_max = emax;
   *dist_sum = total;
   return ORACLE_OK;
+}
+
+/* variants/not_regular_grid_graph/evaluation.c:122-190: the grid level loop
+ * with row i holding degree[i] neighbours (max_degree slots). */
+int oracle_grid_eval_nr(int nodes, int max_degree, const int *degree, int groups, const int *adj, int based_nodes,
+                        const int *rotate_hash, int *diameter, double *ASPL, long long *sum_out)
+{
+  int dp;
+  long long sp;
+  int rc = grid_partial_impl(nodes, max_degree, degree, groups, adj, based_nodes, rotate_hash, 0, 1, &dp, &sp);
+  if (rc) return rc;
+  if (sum_out) *sum_out = sp + (long long)nodes * (nodes - 1);
+  return oracle_grid_finish(nodes, dp, sp, diameter, ASPL);
 }

@@ -80,3 +80,52 @@ def test_grid_sa_trajectory_identical(gpu, tmp_path, w, h, d, r, seed, steps):
     gpu_out = _run("gg_grid_b200", args + ["-o", str(tmp_path / "gpu.edges")], tmp_path)
     assert _stable(cpu) == _stable(gpu_out)
     assert (tmp_path / "cpu.edges").read_text() == (tmp_path / "gpu.edges").read_text()
+
+
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_added_centres_sa_identical(gpu, tmp_path, seed):
+    """-v 16 -g 15 on a 114-vertex 29-regular input: the configuration the
+    reference's own regression log still matches (general/Makefile:78).  The
+    reference's CUDA build refuses -v; its plain build linked against
+    libgg_general.so runs it on the GPU and must equal the CPU build."""
+    _need("gg", "gg_b200_v")
+    gr = graphs.random_regular(114, 29, 100 + seed)
+    f = tmp_path / "in.edges"
+    graphs.write_general(str(f), gr)
+    args = ["-f", str(f), "-s", str(seed), "-n", "100", "-v", "16", "-g", "15"]
+    cpu = _run("gg", args + ["-o", str(tmp_path / "cpu.edges")], tmp_path)
+    gpu_out = _run("gg_b200_v", args + ["-o", str(tmp_path / "gpu.edges")], tmp_path)
+    a, b = _stable(cpu), _stable(gpu_out)
+    assert any("Diam. k" in l for l in a)
+    assert a == b
+    assert (tmp_path / "cpu.edges").read_text() == (tmp_path / "gpu.edges").read_text()
+
+
+def _write_edges(path, edges, height=None):
+    with open(path, "w") as f:
+        for a, b in edges:
+            if height is None:
+                f.write(f"{a} {b}\n")
+            else:
+                f.write(f"{a // height},{a % height} {b // height},{b % height}\n")
+
+
+@pytest.mark.parametrize("halfway,seed", [(True, 1), (False, 2)])
+def test_nonregular_general_sa_identical(gpu, tmp_path, halfway, seed):
+    """The reference's non-regular general program, CPU evaluator against
+    libgg_general_nr.so."""
+    _need("gg_nr", "gg_nr_b200")
+    e, _, _ = graphs.nonregular(graphs.random_regular(512, 8, 5), 200, seed)
+    f = tmp_path / "in.edges"
+    _write_edges(f, e)
+    args = ["-f", str(f), "-s", str(seed), "-n", "300"] + (["-M"] if halfway else [])
+    assert _stable(_run("gg_nr", args, tmp_path)) == _stable(_run("gg_nr_b200", args, tmp_path))
+
+
+def test_nonregular_grid_sa_identical(gpu, tmp_path):
+    _need("gg_grid_nr", "gg_grid_nr_b200")
+    e, _, _ = graphs.nonregular(graphs.grid_regular(16, 16, 6, 3, 4), 100, 2)
+    f = tmp_path / "in.edges"
+    _write_edges(f, e, height=16)
+    args = ["-f", str(f), "-R", "3", "-s", "1", "-n", "200"]
+    assert _stable(_run("gg_grid_nr", args, tmp_path)) == _stable(_run("gg_grid_nr_b200", args, tmp_path))

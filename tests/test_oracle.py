@@ -149,3 +149,28 @@ def test_reference_build_reproduces_its_golden_log(reference_tree, ref_oracle):
     # the ten -v 16 -g 15 finals are the last line of each seed's block in result.txt
     blocks = [finals[i] for i in range(7, len(finals), 8)]
     assert got == blocks[:10]
+
+
+@pytest.mark.parametrize("n,d,drop,g,ac,algo", [(300, 6, 150, 1, 0, 1), (512, 8, 300, 4, 0, 2), (610, 5, 100, 2, 10, 1),
+                                                (1000, 12, 2000, 1, 40, 1)])
+def test_nonregular_port_vs_reference_build(n, d, drop, g, ac, algo):
+    """The non-regular general variant (per-row degrees in the based phase,
+    whole padded rows in the added-centre phase), port vs the reference build."""
+    if not oracle.have_ref_nr():
+        pytest.skip("oracle/_ref non-regular builds absent")
+    gr = graphs.random_regular(n, d, n + drop)
+    _, adj, deg = graphs.nonregular(gr, drop, 7)
+    bn = (n - ac) // g
+    got = oracle.general_nr(adj, deg, based_nodes=bn, groups=g, added_centers=ac, algo=algo)
+    assert got[:3] == oracle.ref_general_nr(adj, deg, based_nodes=bn, groups=g, added_centers=ac, algo=algo)
+
+
+@pytest.mark.parametrize("w,h,d,drop,g", [(16, 16, 6, 100, 1), (20, 20, 4, 60, 2), (18, 18, 6, 120, 4)])
+def test_nonregular_grid_port_vs_reference_build(w, h, d, drop, g):
+    if not oracle.have_ref_nr():
+        pytest.skip("oracle/_ref non-regular builds absent")
+    gr = graphs.grid_regular(w, h, d, 3, w + drop)
+    _, adj, deg = graphs.nonregular(gr, drop, 3)
+    rh = graphs.rotate_hash(gr.nodes, h, w, g)
+    got = oracle.grid_nr(adj, deg, rh, groups=g)
+    assert got[:3] == oracle.ref_grid_nr(adj, deg, rh, groups=g)
