@@ -81,6 +81,17 @@ CORE_SIGNATURES = {
     "ggb_eval_general_noalloc": (_I, [_I, _I, _I, _I, _P, _I, _P, C.POINTER(ggb_result)]),
     "ggb_noalloc_scratch_bytes": (_LL, []),
     "ggb_noalloc_last_error": (C.c_char_p, []),
+    "ggb_batch_create": (_I, [_I, _P, _P, _P, _P, C.POINTER(_P)]),
+    "ggb_batch_destroy": (None, [_P]),
+    "ggb_batch_set_plan": (_I, [_P, _I, _I]),
+    "ggb_batch_get_plan": (_I, [_P, _IP, _IP, _IP]),
+    "ggb_batch_autotune": (_I, [_P, _I, _IP, _IP, C.POINTER(C.c_double)]),
+    "ggb_batch_adj_device": (_I, [_P, _I, C.POINTER(_P)]),
+    "ggb_batch_upload": (_I, [_P, _P, _P]),
+    "ggb_batch_launch": (_I, [_P, _P]),
+    "ggb_batch_collect": (_I, [_P, _P, _P]),
+    "ggb_batch_eval": (_I, [_P, _P, _P]),
+    "ggb_batch_kernel_ms": (_I, [_P, C.POINTER(C.c_double)]),
 }
 
 HOST_SIGNATURES = {

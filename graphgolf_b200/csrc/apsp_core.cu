@@ -24,6 +24,7 @@
 
 #include "../../include/graphgolf_b200.h"
 #include "apsp_kernel.cuh"
+#include "core_internal.h"
 
 namespace ggb {
 
@@ -416,6 +417,24 @@ int read_ctrl(cudaStream_t st, ggb_partial* p) {
 }
 
 cudaStream_t pick_stream(void* s) { return s ? (cudaStream_t)s : g.stream; }
+
+}  // namespace
+
+namespace ggb {
+
+int core_fail(int code, const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof g_err, fmt, ap);
+  va_end(ap);
+  return code;
+}
+
+void core_add_launches(long long n) { g_launches += n; }
+
+}  // namespace ggb
+
+namespace {
 
 int check_general(int nodes, int based_nodes, int groups, int degree, int added_centers) {
   if (nodes <= 0 || based_nodes <= 0 || groups <= 0 || degree < 0 || added_centers < 0)

@@ -630,48 +630,62 @@ __device__ __forceinline__ void sweep_wide(const uint4* __restrict__ src, uint4*
   }
 }
 
-// ---- the persistent kernel -----------------------------------------------------
+// ---- one graph on a team of CTAs ------------------------------------------------
 // R = uint4 words per row (W = 128*R source bits).  LPR lanes share a row,
 // each lane owning UPL uint4 of it; a warp covers VPW vertices per step.
+//
+// eval_windows runs every window of this rank of one graph on the `ncta`
+// CTAs of a team (this CTA is number `cta`), which synchronise through the
+// team's control block a.ctrl.  The single-graph kernel is one team of all
+// CTAs; the batch kernel runs many teams, each over its own list of graphs.
+// bar_target and gl carry over from one graph to the next of a team: the
+// barrier counter and the level-count slots of a.ctrl only grow.  Returns
+// false when a wait ran out or a CTA of the team reported an error (the
+// caller then leaves the kernel).
+struct ApspSmem {
+  unsigned long long red[kWarps][4];
+  unsigned long long seen[4][2];   // must be zero before a team's first graph
+  long long lvl[4];
+  int flag;
+};
+
+struct EvalOut {
+  long long sum, levels, dense_levels;
+  int diam, disconnected, windows;
+};
+
 template <int R>
-__global__ void __launch_bounds__(kThreads, 1) apsp_persistent_kernel(const ApspArgs a) {
+__device__ __forceinline__ bool eval_windows(const ApspArgs& a, int cta, int ncta, ApspSmem& sm, unsigned* s_dyn,
+                                             unsigned long long& bar_target, unsigned& gl, int& ntrace,
+                                             EvalOut& out) {
   constexpr int LPR = R >= 32 ? 32 : R;
   constexpr int VPW = 32 / LPR;
   constexpr int UPL = R / LPR;
   constexpr int W = 128 * R;
   constexpr int U = UPL >= 2 ? 8 : 16;  // neighbour rows in flight per thread
   constexpr int SROW = 4 * R;          // 32-bit words per row in shared memory
-
-  __shared__ unsigned long long s_red[kWarps][4];
-  __shared__ unsigned long long s_seen[4][2];
-  __shared__ long long s_lvl[4];
-  __shared__ int s_flag;
-  extern __shared__ unsigned s_dyn[];   // per warp: neighbour ids [4][64], then rows [4][2][SROW]
+  unsigned long long (*const s_red)[4] = sm.red;
+  unsigned long long (*const s_seen)[2] = sm.seen;
+  long long* const s_lvl = sm.lvl;
 
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   const int sub = lane / LPR;          // which vertex of the warp's VPW
   const int li = lane % LPR;           // lane within the row
-  const long long slot = ((long long)blockIdx.x * kWarps + warp) * VPW + sub;
-  const long long n_slots = (long long)gridDim.x * kWarps * VPW;
+  const long long slot = ((long long)cta * kWarps + warp) * VPW + sub;
+  const long long n_slots = (long long)ncta * kWarps * VPW;
   const int N = a.N, d = a.d;
-  const unsigned grid = gridDim.x;
+  const unsigned grid = (unsigned)ncta;
   int* const my_nb = reinterpret_cast<int*>(s_dyn) + (size_t)warp * (kSeedVerts * kSeedNb + 2 * kSeedVerts * SROW);
   unsigned* const my_rows = reinterpret_cast<unsigned*>(my_nb + kSeedVerts * kSeedNb);
-  const long long warp_id = (long long)blockIdx.x * kWarps + warp;
-  const long long n_warps = (long long)gridDim.x * kWarps;
+  const long long warp_id = (long long)cta * kWarps + warp;
+  const long long n_warps = (long long)ncta * kWarps;
 
-  unsigned long long bar_target = 0;
   // Level counts live in cnt[gl & 3]: between two barriers a CTA adds to the
   // slots of at most two levels while slower CTAs may still read the (at most
   // two) slots of the levels that ended at the previous barrier; four slots
   // keep those sets disjoint.  The counters only grow; s_seen holds the value
   // this CTA read last time, so a level's count is the difference.
-  if (threadIdx.x < 8) s_seen[threadIdx.x >> 1][threadIdx.x & 1] = 0ULL;
-  __syncthreads();
-  unsigned gl = 0;                     // global level counter
-  int ntrace = 0;
-  trace_mark(a, ntrace, 0, 0);
   long long sum = 0, levels = 0, dense_levels = 0;
   int diam = 1, disconnected = 0, windows = 0;
   bool adj_ok = true;
@@ -720,12 +734,12 @@ __global__ void __launch_bounds__(kThreads, 1) apsp_persistent_kernel(const Apsp
         if (!adj_ok) set_error(a.ctrl, kErrAdj, (int)blockIdx.x);
         cta_add_counts<4>(c, a.ctrl, gl, s_red);
         bar_target += grid;
-        if (!grid_barrier(a.ctrl, bar_target + a.phantom, a.timeout_ns, &s_flag)) return;
+        if (!grid_barrier(a.ctrl, bar_target + a.phantom, a.timeout_ns, &sm.flag)) return false;
         trace_mark(a, ntrace, 1, 1);
         read_level_counts(a.ctrl, gl, 2, s_seen, s_lvl);
         const long long seed_lvl[4] = {s_lvl[0], s_lvl[1], s_lvl[2], s_lvl[3]};
         __syncthreads();
-        if (ld_volatile_i32(&a.ctrl->error) != 0) return;
+        if (ld_volatile_i32(&a.ctrl->error) != 0) return false;
         gl += 2;
         ++levels;
         act = level_decision(phase, seed_lvl[0], seed_lvl[1], l, N, lo_rows, hi_rows, a.groups, prev_total, sum);
@@ -808,12 +822,12 @@ __global__ void __launch_bounds__(kThreads, 1) apsp_persistent_kernel(const Apsp
             cta_add_counts<2>(cl, a.ctrl, gl, s_red);
           }
           bar_target += grid;
-          if (!grid_barrier(a.ctrl, bar_target + a.phantom, a.timeout_ns, &s_flag)) return;
+          if (!grid_barrier(a.ctrl, bar_target + a.phantom, a.timeout_ns, &sm.flag)) return false;
           trace_mark(a, ntrace, 2, kk);
           read_level_counts(a.ctrl, gl, own_count ? 2 : 1, s_seen, s_lvl);
           const long long l0 = s_lvl[0], l1 = s_lvl[1], l2 = s_lvl[2], l3 = s_lvl[3];
           __syncthreads();   // s_lvl is rewritten after the next barrier only
-          if (ld_volatile_i32(&a.ctrl->error) != 0) return;   // same answer in every CTA after the barrier
+          if (ld_volatile_i32(&a.ctrl->error) != 0) return false;   // same answer in every CTA after the barrier
           ++dense_levels;
           if (own_count) {
             ++gl;
@@ -839,17 +853,126 @@ __global__ void __launch_bounds__(kThreads, 1) apsp_persistent_kernel(const Apsp
     }
   }
 
+  out.sum = sum;
+  out.levels = levels;
+  out.dense_levels = dense_levels;
+  out.diam = diam;
+  out.disconnected = disconnected;
+  out.windows = windows;
+  return true;
+}
+
+// ---- the single-graph persistent kernel ---------------------------------------
+template <int R>
+__global__ void __launch_bounds__(kThreads, 1) apsp_persistent_kernel(const ApspArgs a) {
+  __shared__ ApspSmem sm;
+  extern __shared__ unsigned s_dyn[];   // per warp: neighbour ids [4][64], then rows [4][2][SROW]
+  if (threadIdx.x < 8) sm.seen[threadIdx.x >> 1][threadIdx.x & 1] = 0ULL;
+  __syncthreads();
+  unsigned long long bar_target = 0;
+  unsigned gl = 0;                     // global level counter
+  int ntrace = 0;
+  trace_mark(a, ntrace, 0, 0);
+  EvalOut o;
+  if (!eval_windows<R>(a, (int)blockIdx.x, (int)gridDim.x, sm, s_dyn, bar_target, gl, ntrace, o)) return;
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     ApspCtrl* c = a.ctrl;
-    c->diam = diam;
-    c->disconnected = disconnected;
-    c->sum = sum;
-    c->levels = levels;
-    c->dense_levels = dense_levels;
-    c->windows = windows;
+    c->diam = o.diam;
+    c->disconnected = o.disconnected;
+    c->sum = o.sum;
+    c->levels = o.levels;
+    c->dense_levels = o.dense_levels;
+    c->windows = o.windows;
     c->trace_len = ntrace;
     __threadfence();
     c->done = 1;
+  }
+}
+
+// ---- the batch kernel: many graphs, one launch -----------------------------------
+// The CTAs of the launch form n_teams teams of team_ctas CTAs (CTAs past the
+// last full team return at once).  Team t evaluates the graphs
+// team_list[team_start[t] .. team_start[t+1]) one after the other, every
+// window of each on all of its CTAs, synchronising through its own control
+// block team_ctrl[t] and keeping its two bitset matrices in its own slice of
+// the scratch.  A graph's answer depends only on its adjacency: the team size
+// and the window width change the schedule, never a count.
+struct BatchGraph {
+  const int* adj;        // [N][d], device
+  int N, d;
+  int n_src;             // phase-1 sources (based_nodes); N = n_src * groups
+  int groups;
+  int vec4;              // d % 4 == 0 and adj 16-byte aligned
+  int pad_;
+};
+
+struct BatchOut {        // per graph, written by the team's first CTA
+  long long sum, levels, dense_levels;
+  int diam, disconnected, windows, done;
+};
+
+struct BatchArgs {
+  const BatchGraph* graphs;
+  BatchOut* out;
+  ApspCtrl* team_ctrl;            // [n_teams], zeroed before the launch
+  const int* team_start;          // [n_teams + 1]
+  const int* team_list;           // graph ids, in run order per team
+  uint4* scratch;
+  const long long* team_off;      // team t: buf0 = scratch + team_off[t], buf1 = buf0 + team_cells[t]
+  const long long* team_cells;
+  long long timeout_ns;
+  int n_teams, team_ctas;
+};
+
+template <int R>
+__global__ void __launch_bounds__(kThreads, 1) apsp_batch_kernel(const BatchArgs b) {
+  __shared__ ApspSmem sm;
+  extern __shared__ unsigned s_dyn[];
+  const int team = (int)blockIdx.x / b.team_ctas;
+  const int cta = (int)blockIdx.x % b.team_ctas;
+  if (team >= b.n_teams) return;
+  if (threadIdx.x < 8) sm.seen[threadIdx.x >> 1][threadIdx.x & 1] = 0ULL;
+  __syncthreads();
+  ApspArgs a;
+  a.adj2 = nullptr;
+  a.buf0 = b.scratch + b.team_off[team];
+  a.buf1 = a.buf0 + b.team_cells[team];
+  a.ctrl = b.team_ctrl + team;
+  a.timeout_ns = b.timeout_ns;
+  a.ac = 0;
+  a.win_first = 0;
+  a.win_stride = 1;
+  a.ball = nullptr;
+  a.ball_cnt = nullptr;
+  a.trace = nullptr;
+  a.trace_cap = 0;
+  a.phantom = 0;
+  unsigned long long bar_target = 0;
+  unsigned gl = 0;
+  int ntrace = 0;
+  const int k1 = b.team_start[team + 1];
+  for (int k = b.team_start[team]; k < k1; ++k) {
+    const int gi = b.team_list[k];
+    const BatchGraph gr = b.graphs[gi];
+    a.adj = gr.adj;
+    a.N = gr.N;
+    a.d = gr.d;
+    a.n_src1 = gr.n_src;
+    a.split = gr.N;
+    a.groups = gr.groups;
+    a.vec4 = gr.vec4;
+    EvalOut o;
+    if (!eval_windows<R>(a, cta, b.team_ctas, sm, s_dyn, bar_target, gl, ntrace, o)) return;
+    if (cta == 0 && threadIdx.x == 0) {
+      BatchOut* w = b.out + gi;
+      w->sum = o.sum;
+      w->levels = o.levels;
+      w->dense_levels = o.dense_levels;
+      w->diam = o.diam;
+      w->disconnected = o.disconnected;
+      w->windows = o.windows;
+      w->done = 1;
+    }
   }
 }
 

@@ -155,3 +155,43 @@ def nonregular(g: Graph, drop: int, seed: int, pad: int = -1) -> tuple[np.ndarra
         deg[b] += 1
     return edges, adj, deg
 
+
+
+def swap_2opt(g: Graph, seed: int, tries: int = 10000) -> Graph:
+    """One seeded 2-opt edge swap of g (the move of general/sa.c:217-369 with
+    groups = 1): lines i != j, (a,b),(c,d) become (a,c),(b,d) or (a,d),(b,c),
+    redrawn until the result has no self-loop and no repeated edge."""
+    rng = np.random.default_rng(seed)
+    e = np.array(g.edges, dtype=np.int32, copy=True)
+    for _ in range(tries):
+        i, j = (int(x) for x in rng.integers(0, g.lines, 2))
+        if i == j:
+            continue
+        a, b = (int(x) for x in e[i])
+        c, d = (int(x) for x in e[j])
+        (p, q), (r, s) = ((a, c), (b, d)) if rng.integers(2) else ((a, d), (b, c))
+        if p == q or r == s or {p, q} == {r, s}:
+            continue
+        if q in g.adj[p] or s in g.adj[r]:
+            continue
+        e[i] = (p, q)
+        e[j] = (r, s)
+        return Graph(g.nodes, g.degree, e, create_adj(g.nodes, g.degree, e), groups=g.groups)
+    raise ValueError("swap_2opt: no valid swap found")
+
+
+def batch_workload(candidates: int = 256, degree: int = 12, n_lo: int = 512, n_hi: int = 16384,
+                   base_nodes: int = 4096, seed: int = 1) -> list[Graph]:
+    """A mixed batch: a random degree-regular base graph of base_nodes
+    vertices, then `candidates` graphs, each one seeded 2-opt swap of its own
+    random degree-regular base graph whose vertex count is drawn
+    log-uniformly from [n_lo, n_hi]."""
+    rng = np.random.default_rng(seed)
+    out = [random_regular(base_nodes, degree, seed)]
+    for k in range(candidates):
+        n = int(round(float(np.exp(rng.uniform(np.log(n_lo), np.log(n_hi))))))
+        if (n * degree) % 2:
+            n += 1
+        s = seed * 1000003 + k + 1
+        out.append(swap_2opt(random_regular(n, degree, s), s))
+    return out

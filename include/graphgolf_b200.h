@@ -228,6 +228,57 @@ int ggb_finish_general(int nodes, const ggb_partial *reduced, ggb_result *out);
  * (grid/evaluation.c:176-189). */
 int ggb_finish_grid(int nodes, const ggb_partial *reduced, ggb_result *out);
 
+/* ---- batches: many graphs, of uneven sizes, in one launch --------------- */
+
+/* A batch is a fixed list of general graphs (ac = 0) whose adjacency arrays
+ * live packed in one device buffer; one cooperative launch, captured once in a
+ * CUDA graph and replayed, evaluates them all.  Its CTAs form teams of
+ * team_ctas CTAs; the graphs are dealt to the teams longest-first; every team
+ * runs its graphs' source windows of window_bits sources with a barrier of its
+ * own.  Each graph's result is the one ggb_eval_general gives it
+ * (general/evaluation.c:153-263 per graph, :249-262 for the convention).  No
+ * counterpart in the reference, whose evaluation() takes one graph.
+ * A batch belongs to the device current at ggb_batch_create; it is not
+ * thread-safe. */
+typedef struct ggb_batch ggb_batch;
+
+/* Creates a batch of n_graphs graphs; graph i has nodes[i] vertices,
+ * based_nodes[i] * groups[i] == nodes[i], degree[i] neighbours per row.  The
+ * initial plan is the cost model's choice. */
+int ggb_batch_create(int n_graphs, const int *nodes, const int *based_nodes, const int *groups,
+                     const int *degree, ggb_batch **out);
+void ggb_batch_destroy(ggb_batch *b);
+
+/* Fixes the plan: window_bits = 128 * 2^k (<= 4096), team_ctas >= 1; a 0
+ * leaves that choice to the cost model. */
+int ggb_batch_set_plan(ggb_batch *b, int window_bits, int team_ctas);
+int ggb_batch_get_plan(const ggb_batch *b, int *window_bits, int *team_ctas, int *teams);
+
+/* Times every feasible (window_bits, team_ctas) pair on the batch's current
+ * adjacency (iters timed launches each, after one warm-up) and keeps the
+ * fastest; reports it and its time. */
+int ggb_batch_autotune(ggb_batch *b, int iters, int *window_bits, int *team_ctas, double *best_ms);
+
+/* Device address of graph i's [nodes][degree] adjacency inside the batch
+ * (16-byte aligned), for producers that write candidates on the device. */
+int ggb_batch_adj_device(ggb_batch *b, int graph, int **adj_dev);
+
+/* Copies host adjacency arrays adj[0..n_graphs) into the batch (on `stream`,
+ * or the batch's own stream when NULL). */
+int ggb_batch_upload(ggb_batch *b, const int *const *adj, void *stream);
+
+/* Enqueues the evaluation of the batch's device adjacency on `stream` (NULL:
+ * the batch's own stream); ggb_batch_collect waits and writes results[i]
+ * (results may be NULL to only check for errors). */
+int ggb_batch_launch(ggb_batch *b, void *stream);
+int ggb_batch_collect(ggb_batch *b, void *stream, ggb_result *results);
+
+/* Upload + launch + collect. */
+int ggb_batch_eval(ggb_batch *b, const int *const *adj, ggb_result *results);
+
+/* Device time of the last collected launch (CUDA events around it). */
+int ggb_batch_kernel_ms(const ggb_batch *b, double *ms);
+
 #ifdef __cplusplus
 }
 #endif
