@@ -6,13 +6,14 @@ grid/evaluation.c:122-190), rebuilt as a persistent sm_100a CUDA kernel
 behind the reference's own C ``evaluation()`` interface.
 """
 from ._native import NativeLibraryMissing, load
+from .anneal import Annealer, FilterNet
 from .batch import Batch
 from .evaluator import (BFS, MATRIX_OP, MATRIX_OP_MEM_SAVING, EvaluationError, Result, evaluate,
                         evaluate_grid, evaluate_grid_nonregular, evaluate_nonregular, evaluate_partial, evaluation, finish_general, grid_evaluation,
                         kernel_launches, set_ball, set_tuning)
 
 __all__ = [
-    "BFS", "Batch", "MATRIX_OP", "MATRIX_OP_MEM_SAVING", "EvaluationError", "NativeLibraryMissing", "Result",
+    "Annealer", "BFS", "Batch", "FilterNet", "MATRIX_OP", "MATRIX_OP_MEM_SAVING", "EvaluationError", "NativeLibraryMissing", "Result",
     "evaluate", "evaluate_grid", "evaluate_grid_nonregular", "evaluate_nonregular", "evaluate_partial", "evaluation", "finish_general", "grid_evaluation",
     "kernel_launches", "load", "set_ball", "set_tuning",
 ]

@@ -48,6 +48,27 @@ class ggb_partial(C.Structure):
     ]
 
 
+class ggb_sa_stats(C.Structure):
+    """Mirror of ``ggb_sa_stats`` in include/graphgolf_b200.h."""
+
+    _fields_ = [
+        ("step", C.c_longlong),
+        ("accepts", C.c_longlong),
+        ("multi_accepts", C.c_longlong),
+        ("moved_swaps", C.c_longlong),
+        ("evals", C.c_longlong),
+        ("pred_accepts", C.c_longlong),
+        ("cur_diam", C.c_int),
+        ("best_diam", C.c_int),
+        ("cur_total", C.c_longlong),
+        ("best_total", C.c_longlong),
+        ("cur_aspl", C.c_double),
+        ("best_aspl", C.c_double),
+        ("temp", C.c_double),
+        ("done", C.c_int),
+    ]
+
+
 _I = C.c_int
 _LL = C.c_longlong
 _P = C.c_void_p
@@ -92,6 +113,24 @@ CORE_SIGNATURES = {
     "ggb_batch_collect": (_I, [_P, _P, _P]),
     "ggb_batch_eval": (_I, [_P, _P, _P]),
     "ggb_batch_kernel_ms": (_I, [_P, C.POINTER(C.c_double)]),
+    "ggb_mlp_create": (_I, [_I, C.c_ulonglong, C.POINTER(_P)]),
+    "ggb_mlp_destroy": (None, [_P]),
+    "ggb_mlp_param_count": (_I, []),
+    "ggb_mlp_set_params": (_I, [_P, _P]),
+    "ggb_mlp_get_params": (_I, [_P, _P]),
+    "ggb_mlp_set_adam": (_I, [_P, C.c_float, C.c_float, C.c_float, C.c_float]),
+    "ggb_mlp_forward_host": (_I, [_P, _P, _I, _P]),
+    "ggb_mlp_grads_host": (_I, [_P, _P, _P, _I, _P, _P]),
+    "ggb_mlp_train_host": (_I, [_P, _P, _P, _I, _I, _P]),
+    "ggb_sa_create": (_I, [_I, _I, _P, _I, _I, _I, C.c_ulonglong, C.POINTER(_P)]),
+    "ggb_sa_destroy": (None, [_P]),
+    "ggb_sa_set_schedule": (_I, [_P, C.c_double, C.c_double, _I]),
+    "ggb_sa_set_target": (_I, [_P, _I, _LL]),
+    "ggb_sa_autotune": (_I, [_P, _I, _IP, _IP, C.POINTER(C.c_double)]),
+    "ggb_sa_run": (_I, [_P, _LL, C.POINTER(ggb_sa_stats)]),
+    "ggb_sa_edges": (_I, [_P, _I, _P]),
+    "ggb_sa_profile": (_I, [_P, _P]),
+    "ggb_sa_last_step": (_I, [_P, _P, _P]),
 }
 
 HOST_SIGNATURES = {

@@ -1,0 +1,172 @@
+"""Simulated annealing with the whole step on the device, and its learned
+proposal filter.
+
+``Annealer`` wraps the ``ggb_sa_*`` C ABI (include/graphgolf_b200.h): every
+step draws 2-opt swaps of the current graph, optionally ranks them with the
+filter network, evaluates the best ones exactly in one batch launch, composes
+the disjoint improving ones into one more exactly evaluated graph and accepts
+by the reference's rule (general/sa.c:371-411).  ``candidates=1`` without
+composition is the reference's plain step (general/sa.c:413-520) on the
+device.  ``FilterNet`` exposes the filter's network (ggb_mlp_*) on its own.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from ._native import ggb_sa_stats, load
+from .evaluator import _raise
+from .graphs import Graph
+
+
+@dataclass(frozen=True)
+class Stats:
+    step: int
+    accepts: int
+    multi_accepts: int
+    moved_swaps: int
+    evals: int
+    pred_accepts: int
+    cur_diam: int
+    best_diam: int
+    cur_total: int
+    best_total: int
+    cur_aspl: float
+    best_aspl: float
+    temp: float
+    done: bool
+
+
+class Annealer:
+    def __init__(self, g: Graph, candidates: int = 1, proposals: int | None = None, compose: int = 0,
+                 seed: int = 1):
+        if g.groups != 1:
+            raise ValueError("device annealing takes graphs without symmetry groups")
+        self._lib = load()
+        self.nodes, self.degree, self.lines = g.nodes, g.degree, g.lines
+        self.candidates = candidates
+        e = np.ascontiguousarray(g.edges, dtype=np.int32)
+        h = C.c_void_p()
+        _raise(self._lib.ggb_sa_create(g.nodes, g.degree, e.ctypes.data, candidates,
+                                       proposals if proposals else candidates, compose, seed, C.byref(h)))
+        self._h = h
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.ggb_sa_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self) -> "Annealer":
+        return self
+
+    def __exit__(self, *exc) -> None:
+        self.close()
+
+    def schedule(self, temp: float = 0.0, cooling: float = 1.0, hill_climbing: bool = True) -> None:
+        _raise(self._lib.ggb_sa_set_schedule(self._h, temp, cooling, 1 if hill_climbing else 0))
+
+    def target(self, diameter: int, total: int) -> None:
+        _raise(self._lib.ggb_sa_set_target(self._h, diameter, total))
+
+    def autotune(self, iters: int = 1) -> tuple[int, int, float]:
+        w, t, ms = C.c_int(), C.c_int(), C.c_double()
+        _raise(self._lib.ggb_sa_autotune(self._h, iters, C.byref(w), C.byref(t), C.byref(ms)))
+        return w.value, t.value, ms.value
+
+    def run(self, steps: int) -> Stats:
+        st = ggb_sa_stats()
+        _raise(self._lib.ggb_sa_run(self._h, steps, C.byref(st)))
+        return Stats(st.step, st.accepts, st.multi_accepts, st.moved_swaps, st.evals, st.pred_accepts, st.cur_diam,
+                     st.best_diam,
+                     st.cur_total, st.best_total, st.cur_aspl, st.best_aspl, st.temp, bool(st.done))
+
+    def edges(self, best: bool = False) -> np.ndarray:
+        out = np.empty((self.lines, 2), dtype=np.int32)
+        _raise(self._lib.ggb_sa_edges(self._h, 1 if best else 0, out.ctypes.data))
+        return out
+
+    def last_step(self) -> tuple[np.ndarray, np.ndarray]:
+        """(predicted, exact label) of the last step's evaluated candidates."""
+        k = self.candidates
+        pr = np.empty(k, dtype=np.float32)
+        lb = np.empty(k, dtype=np.float32)
+        _raise(self._lib.ggb_sa_last_step(self._h, pr.ctypes.data, lb.ctypes.data))
+        return pr, lb
+
+    def profile(self) -> np.ndarray:
+        """[nodes][32]: entry [v][k] = vertices farther than k from v."""
+        out = np.empty((self.nodes, 32), dtype=np.uint32)
+        _raise(self._lib.ggb_sa_profile(self._h, out.ctypes.data))
+        return out
+
+
+class FilterNet:
+    """The proposal filter's network: 32 -> 256 -> 256 -> 1 ReLU MLP, BF16
+    tensor cores with FP32 accumulation, Adam on the mean squared error."""
+
+    FEATURES, HIDDEN = 32, 256
+
+    def __init__(self, max_rows: int = 4096, seed: int = 1):
+        self._lib = load()
+        h = C.c_void_p()
+        _raise(self._lib.ggb_mlp_create(max_rows, seed, C.byref(h)))
+        self._h = h
+        self.n_params = int(self._lib.ggb_mlp_param_count())
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.ggb_mlp_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def params(self) -> np.ndarray:
+        p = np.empty(self.n_params, dtype=np.float32)
+        _raise(self._lib.ggb_mlp_get_params(self._h, p.ctypes.data))
+        return p
+
+    @params.setter
+    def params(self, p) -> None:
+        a = np.ascontiguousarray(p, dtype=np.float32)
+        if a.size != self.n_params:
+            raise ValueError(f"expected {self.n_params} parameters")
+        _raise(self._lib.ggb_mlp_set_params(self._h, a.ctypes.data))
+
+    def set_adam(self, lr: float = 1e-3, beta1: float = 0.9, beta2: float = 0.999, eps: float = 1e-8) -> None:
+        _raise(self._lib.ggb_mlp_set_adam(self._h, lr, beta1, beta2, eps))
+
+    def forward(self, x) -> np.ndarray:
+        a = np.ascontiguousarray(x, dtype=np.float32)
+        y = np.empty(a.shape[0], dtype=np.float32)
+        _raise(self._lib.ggb_mlp_forward_host(self._h, a.ctypes.data, a.shape[0], y.ctypes.data))
+        return y
+
+    def grads(self, x, t) -> tuple[float, np.ndarray]:
+        a = np.ascontiguousarray(x, dtype=np.float32)
+        b = np.ascontiguousarray(t, dtype=np.float32)
+        g = np.empty(self.n_params, dtype=np.float32)
+        loss = C.c_float()
+        _raise(self._lib.ggb_mlp_grads_host(self._h, a.ctypes.data, b.ctypes.data, a.shape[0], C.byref(loss),
+                                            g.ctypes.data))
+        return loss.value, g
+
+    def train(self, x, t, steps: int) -> float:
+        a = np.ascontiguousarray(x, dtype=np.float32)
+        b = np.ascontiguousarray(t, dtype=np.float32)
+        loss = C.c_float()
+        _raise(self._lib.ggb_mlp_train_host(self._h, a.ctypes.data, b.ctypes.data, a.shape[0], steps,
+                                            C.byref(loss)))
+        return loss.value

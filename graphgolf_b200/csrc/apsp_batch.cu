@@ -29,6 +29,7 @@
 
 #include "../../include/graphgolf_b200.h"
 #include "apsp_kernel.cuh"
+#include "batch_internal.h"
 #include "core_internal.h"
 
 using ggb::core_fail;
@@ -86,41 +87,6 @@ int dev_alloc(T** p, size_t n) {
 }
 
 }  // namespace
-
-struct ggb_batch {
-  int device = -1;
-  int sms = 0;
-  size_t l2 = 0;
-  int n = 0;
-  std::vector<int> N, bn, grp, d;
-  std::vector<long long> off;        // ints; every graph starts on a 16-byte boundary
-  long long adj_ints = 0;
-  int* d_adj = nullptr;
-  int* h_adj = nullptr;              // pinned staging for ggb_batch_eval
-  ggb::BatchGraph* d_graphs = nullptr;
-  ggb::BatchOut* d_out = nullptr;
-  ggb::BatchOut* h_out = nullptr;
-  // the plan
-  int R = 0, T = 0, n_teams = 0, ctas = 0;
-  std::vector<int> team_start, team_list;
-  std::vector<long long> team_off, team_cells;
-  ggb::ApspCtrl* d_ctrl = nullptr;   // [max_teams]
-  ggb::ApspCtrl* h_ctrl = nullptr;
-  int* d_tstart = nullptr;           // [max_teams + 1]
-  int* d_tlist = nullptr;            // [n]
-  long long* d_toff = nullptr;       // [max_teams]
-  long long* d_tcells = nullptr;     // [max_teams]
-  uint4* d_scratch = nullptr;
-  size_t cap_scratch = 0;            // uint4
-  int occ[6] = {0, 0, 0, 0, 0, 0};   // co-resident batch CTAs per SM, per log2(R)
-  int max_teams = 0;                 // largest CTA count of any plan
-  long long timeout_ns = 2000000000LL;
-  cudaStream_t stream = nullptr;
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t exec = nullptr;
-  cudaEvent_t ev[2] = {nullptr, nullptr};
-  bool pending = false;
-};
 
 namespace {
 
@@ -241,13 +207,17 @@ ggb::BatchArgs batch_args(const ggb_batch* b) {
   a.team_off = b->d_toff;
   a.team_cells = b->d_tcells;
   a.timeout_ns = b->timeout_ns;
+  a.stop = b->stop;
+  a.sticky = b->sticky;
   a.n_teams = b->n_teams;
   a.team_ctas = b->T;
   return a;
 }
 
+}  // namespace
+
 // The launch itself: zero the control blocks and results, then the kernel.
-int enqueue(ggb_batch* b, cudaStream_t st) {
+int ggb::batch_enqueue(ggb_batch* b, cudaStream_t st) {
   BCUDA(cudaMemsetAsync(b->d_ctrl, 0, (size_t)b->n_teams * sizeof(ggb::ApspCtrl), st));
   BCUDA(cudaMemsetAsync(b->d_out, 0, (size_t)b->n * sizeof(ggb::BatchOut), st));
   ggb::BatchArgs args = batch_args(b);
@@ -266,10 +236,12 @@ int enqueue(ggb_batch* b, cudaStream_t st) {
   return GGB_OK;
 }
 
+namespace {
+
 int capture(ggb_batch* b) {
   if (b->exec) return GGB_OK;
   BCUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-  int rc = enqueue(b, b->stream);
+  int rc = ggb::batch_enqueue(b, b->stream);
   cudaGraph_t gph = nullptr;
   const cudaError_t e = cudaStreamEndCapture(b->stream, &gph);
   if (rc) {
@@ -293,7 +265,7 @@ int launch(ggb_batch* b, cudaStream_t st, bool use_graph) {
     if (rc) return rc;
     BCUDA(cudaGraphLaunch(b->exec, st));
   } else {
-    int rc = enqueue(b, st);
+    int rc = ggb::batch_enqueue(b, st);
     if (rc) return rc;
   }
   BCUDA(cudaEventRecord(b->ev[1], st));

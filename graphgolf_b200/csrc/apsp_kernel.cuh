@@ -47,6 +47,7 @@ constexpr int kWarps = kThreads / 32;
 constexpr int kBallThreads = 256;     // threads per CTA of the ball pre-pass
 constexpr int kBallMaxWindows = 32;   // windows of one rank in the ball pre-pass (one per lane)
 constexpr int kBallMaxDegree = 32;
+constexpr int kStatLevels = 32;       // levels the per-vertex statistics keep (profile kernel)
 
 // Error codes written to ApspCtrl::error (host maps them to GGB_E*).
 enum : int { kErrNone = 0, kErrAdj = 1, kErrTimeout = 2, kErrPerm = 3, kErrDegree = 4 };
@@ -89,6 +90,7 @@ struct ApspArgs {
   int trace_cap;         // pairs available in trace
   int phantom;           // extra arrivals every barrier waits for: 0 in normal use; the
                          // fault-path test sets 1 so that every bounded wait runs out
+  unsigned* stats;       // profile kernel only: [N][kStatLevels] unreached sources per level
 };
 
 __device__ __forceinline__ unsigned long long globaltimer_ns() {
@@ -385,7 +387,7 @@ constexpr int kSeedNb = 64;                      // neighbour ids staged per ver
 // set the bits of every two-hop vertex; the warp then writes the 4 S_2 rows
 // out coalesced.  Replaces the reference's clear + identity set-up (:168-172)
 // and its first two OR-gather sweeps.
-template <int R, int VEC>
+template <int R, int VEC, bool STATS = false>
 __device__ __forceinline__ void seed_window(const ApspArgs& a, const int* __restrict__ adj, int base, int l,
                                             uint4* s2_out, int* s_nb,
                                             unsigned* s_rw, unsigned (&c)[4], bool& adj_ok, long long warp_id,
@@ -432,6 +434,15 @@ __device__ __forceinline__ void seed_window(const ApspArgs& a, const int* __rest
         c2 += popc4(x2);
       }
       if (vi < a.split) { c[0] += c1; c[2] += c2; } else { c[1] += c1; c[3] += c2; }
+      if constexpr (STATS) {
+        const unsigned t1 = __reduce_add_sync(0xffffffffu, c1), t2 = __reduce_add_sync(0xffffffffu, c2);
+        if (lane == 0) {
+          unsigned* st = a.stats + vi * kStatLevels;
+          st[0] += (unsigned)l - ((unsigned)(vi - base) < (unsigned)l ? 1u : 0u);
+          st[1] += (unsigned)l - t1;
+          st[2] += (unsigned)l - t2;
+        }
+      }
     }
     __syncwarp();
   }
@@ -564,11 +575,11 @@ __device__ __forceinline__ bool equal4(const uint4& a, const uint4& b) {
 // vertex's own row is already full (every valid bit set) loads nothing: the OR
 // cannot change it.  Near the last level, when most rows are almost full,
 // this drops most of the gathered sectors.
-template <int R>
+template <int R, bool STATS = false>
 __device__ __forceinline__ void sweep_wide(const uint4* __restrict__ src, uint4* __restrict__ dst,
                                            const int* __restrict__ adj, int N, int d, int split, long long v0,
                                            long long stride, int l, bool own_count, unsigned (&cl)[4],
-                                           bool& adj_ok) {
+                                           bool& adj_ok, unsigned* stats = nullptr, int lvl = 0) {
   constexpr int UPL = R / 32;
   constexpr int U = UPL >= 2 ? 8 : 16;
   const int lane = threadIdx.x & 31;
@@ -627,6 +638,10 @@ __device__ __forceinline__ void sweep_wide(const uint4* __restrict__ src, uint4*
       cc += popc4(acc[k]);
     }
     if (v < split) cl[0] += cc; else cl[1] += cc;
+    if constexpr (STATS) {
+      const unsigned tot = __reduce_add_sync(0xffffffffu, cc);
+      if (lane == 0 && lvl < kStatLevels) stats[v * kStatLevels + lvl] += (unsigned)l - tot;
+    }
   }
 }
 
@@ -654,7 +669,7 @@ struct EvalOut {
   int diam, disconnected, windows;
 };
 
-template <int R>
+template <int R, bool STATS = false>
 __device__ __forceinline__ bool eval_windows(const ApspArgs& a, int cta, int ncta, ApspSmem& sm, unsigned* s_dyn,
                                              unsigned long long& bar_target, unsigned& gl, int& ntrace,
                                              EvalOut& out) {
@@ -728,9 +743,9 @@ __device__ __forceinline__ bool eval_windows(const ApspArgs& a, int cta, int nct
         // ---- levels 0 and 1 by two-hop seeding into buf0 -----------------------
         unsigned c[4] = {0u, 0u, 0u, 0u};  // S_1 lo, S_1 hi, S_2 lo, S_2 hi
         if (a.vec4)
-          seed_window<R, 4>(a, adjp, base, l, a.buf0, my_nb, my_rows, c, adj_ok, warp_id, n_warps);
+          seed_window<R, 4, STATS>(a, adjp, base, l, a.buf0, my_nb, my_rows, c, adj_ok, warp_id, n_warps);
         else
-          seed_window<R, 1>(a, adjp, base, l, a.buf0, my_nb, my_rows, c, adj_ok, warp_id, n_warps);
+          seed_window<R, 1, STATS>(a, adjp, base, l, a.buf0, my_nb, my_rows, c, adj_ok, warp_id, n_warps);
         if (!adj_ok) set_error(a.ctrl, kErrAdj, (int)blockIdx.x);
         cta_add_counts<4>(c, a.ctrl, gl, s_red);
         bar_target += grid;
@@ -766,7 +781,8 @@ __device__ __forceinline__ bool eval_windows(const ApspArgs& a, int cta, int nct
           if constexpr (LPR == 32) {
             if (d <= 32 && !own_count && prev_total * 10 >= (long long)N * l * 9) {
               wide = true;
-              sweep_wide<R>(src, dst, adjp, N, d, a.split, slot, n_slots, l, own_count, cl, adj_ok);
+              sweep_wide<R, STATS>(src, dst, adjp, N, d, a.split, slot, n_slots, l, own_count, cl, adj_ok,
+                                   a.stats, (int)kk + 1);
             }
           }
           for (long long v = wide ? N : slot; v < N; v += n_slots) {
@@ -812,6 +828,14 @@ __device__ __forceinline__ bool eval_windows(const ApspArgs& a, int cta, int nct
               cc += popc4(acc[k]);
             }
             if (v < a.split) cl[0] += cc; else cl[1] += cc;
+            if constexpr (STATS) {
+              // the LPR lanes of this row hold its popcount in parts
+              const unsigned gmask = LPR == 32 ? 0xffffffffu : (((1u << LPR) - 1u) << (sub * LPR));
+              unsigned tot = cc;
+#pragma unroll
+              for (int o = LPR / 2; o > 0; o >>= 1) tot += __shfl_xor_sync(gmask, tot, o);
+              if (li == 0 && kk + 1 < kStatLevels) a.stats[v * kStatLevels + kk + 1] += (unsigned)l - tot;
+            }
           }
           if (!adj_ok) set_error(a.ctrl, kErrAdj, (int)blockIdx.x);
           if (own_count) {
@@ -921,6 +945,8 @@ struct BatchArgs {
   const long long* team_off;      // team t: buf0 = scratch + team_off[t], buf1 = buf0 + team_cells[t]
   const long long* team_cells;
   long long timeout_ns;
+  const int* stop;                // when non-null and *stop != 0 the launch does nothing
+  int* sticky;                    // when non-null: receives the first team's error code (never cleared here)
   int n_teams, team_ctas;
 };
 
@@ -931,6 +957,7 @@ __global__ void __launch_bounds__(kThreads, 1) apsp_batch_kernel(const BatchArgs
   const int team = (int)blockIdx.x / b.team_ctas;
   const int cta = (int)blockIdx.x % b.team_ctas;
   if (team >= b.n_teams) return;
+  if (b.stop && ld_volatile_i32(b.stop) != 0) return;   // written before the launch: the same in every CTA
   if (threadIdx.x < 8) sm.seen[threadIdx.x >> 1][threadIdx.x & 1] = 0ULL;
   __syncthreads();
   ApspArgs a;
@@ -947,6 +974,7 @@ __global__ void __launch_bounds__(kThreads, 1) apsp_batch_kernel(const BatchArgs
   a.trace = nullptr;
   a.trace_cap = 0;
   a.phantom = 0;
+  a.stats = nullptr;
   unsigned long long bar_target = 0;
   unsigned gl = 0;
   int ntrace = 0;
@@ -962,7 +990,10 @@ __global__ void __launch_bounds__(kThreads, 1) apsp_batch_kernel(const BatchArgs
     a.groups = gr.groups;
     a.vec4 = gr.vec4;
     EvalOut o;
-    if (!eval_windows<R>(a, cta, b.team_ctas, sm, s_dyn, bar_target, gl, ntrace, o)) return;
+    if (!eval_windows<R>(a, cta, b.team_ctas, sm, s_dyn, bar_target, gl, ntrace, o)) {
+      if (b.sticky && threadIdx.x == 0) atomicCAS(b.sticky, 0, max(1, ld_volatile_i32(&a.ctrl->error)));
+      return;
+    }
     if (cta == 0 && threadIdx.x == 0) {
       BatchOut* w = b.out + gi;
       w->sum = o.sum;
@@ -973,6 +1004,47 @@ __global__ void __launch_bounds__(kThreads, 1) apsp_batch_kernel(const BatchArgs
       w->windows = o.windows;
       w->done = 1;
     }
+  }
+}
+
+// ---- the profile kernel: one graph plus per-vertex level statistics -------------
+// stats[v][k] = number of sources not yet reached from v after k levels,
+// summed over all windows (kStatLevels levels kept; the window's rows are
+// complete once a window stops, so later levels add nothing).  From it:
+// eccentricity(v) = first k with stats[v][k] == 0, transmission(v) =
+// sum_k stats[v][k], and the level histogram stats[v][k-1] - stats[v][k].
+// Runs only when *gate != 0 (the annealing engine re-profiles its current
+// graph after an accepted move); the statistics are zeroed here, then the
+// graph is evaluated exactly as the persistent kernel does it, without the
+// ball pre-pass.  A failure also sets *sticky (when given).
+template <int R>
+__global__ void __launch_bounds__(kThreads, 1) apsp_profile_kernel(const ApspArgs a, const int* gate, int* sticky) {
+  __shared__ ApspSmem sm;
+  extern __shared__ unsigned s_dyn[];
+  if (gate && ld_volatile_i32(gate) == 0) return;   // written before the launch: every CTA sees the same value
+  const long long n = (long long)a.N * kStatLevels;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    a.stats[i] = 0u;
+  if (threadIdx.x < 8) sm.seen[threadIdx.x >> 1][threadIdx.x & 1] = 0ULL;
+  unsigned long long bar_target = gridDim.x;
+  unsigned gl = 0;
+  int ntrace = 0;
+  EvalOut o;
+  if (!grid_barrier(a.ctrl, bar_target, a.timeout_ns, &sm.flag) ||
+      !eval_windows<R, true>(a, (int)blockIdx.x, (int)gridDim.x, sm, s_dyn, bar_target, gl, ntrace, o)) {
+    if (sticky && threadIdx.x == 0) atomicCAS(sticky, 0, max(1, ld_volatile_i32(&a.ctrl->error)));
+    return;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    ApspCtrl* c = a.ctrl;
+    c->diam = o.diam;
+    c->disconnected = o.disconnected;
+    c->sum = o.sum;
+    c->levels = o.levels;
+    c->dense_levels = o.dense_levels;
+    c->windows = o.windows;
+    __threadfence();
+    c->done = 1;
   }
 }
 

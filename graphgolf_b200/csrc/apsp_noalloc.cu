@@ -173,6 +173,7 @@ extern "C" int ggb_eval_general_noalloc(int nodes, int based_nodes, int groups, 
   a.trace = nullptr;
   a.trace_cap = 0;
   a.phantom = 0;
+  a.stats = nullptr;
 
   const int lpr = R >= 32 ? 32 : R;
   const int vpw = 32 / lpr;

@@ -1,0 +1,1098 @@
+// sa_device.cu -- simulated annealing with the whole step on the device.
+//
+// The reference's annealing (general/sa.c:413-520) is a host loop: draw one
+// 2-opt swap (exchange_edge_2opt, :217-369), evaluate the graph, accept or
+// reject (accept, :371-411), cool.  Here a step is one replay of a CUDA graph
+// and never returns to the host:
+//
+//   gen        K (or G) candidate swaps of the current graph, each checked in
+//              O(degree) against the current adjacency (no self-loop, no
+//              repeated edge -- the reference's simple-graph rule);
+//   [learned]  features of every candidate from the last exact profile of the
+//              current graph, the MLP's predicted change of the distance
+//              total, and the K best predictions (plus a few random ones) kept;
+//   materialize  the K candidate adjacencies (the current one with 4 entries
+//              changed) into the slots of a batch;
+//   evaluate   all K exactly in one batch launch;
+//   compose    the strictly improving candidates with disjoint endpoints,
+//              best first, applied together to one more graph, which is
+//              evaluated exactly too;
+//   decide     the better of the best single candidate and the composite,
+//              accepted by the reference's rule (smaller diameter; equal
+//              diameter and ASPL not worse; else exp(diff/temp) > uniform);
+//              the swaps are applied to the current graph in place;
+//   [learned]  the K exact changes train the MLP (one Adam step), and an
+//              accepted move re-profiles the current graph for the features.
+//
+// Plain annealing is K = 1 without composition: the reference's step, on the
+// device.  Every acceptance is decided on exact values.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cfloat>
+#include <climits>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+#include "../../include/graphgolf_b200.h"
+#include "batch_internal.h"
+#include "core_internal.h"
+#include "mlp_internal.h"
+
+using ggb::core_fail;
+
+#define SCUDA(call)                                                                                  \
+  do {                                                                                               \
+    cudaError_t e_ = (call);                                                                         \
+    if (e_ != cudaSuccess)                                                                           \
+      return core_fail(GGB_ECUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, \
+                       __LINE__);                                                                    \
+  } while (0)
+
+namespace ggb {
+namespace sa {
+
+using bf16 = __nv_bfloat16;
+
+// One 2-opt swap in canonical form: lines line[0] = {x0,x1} and
+// line[1] = {x2,x3} become {x0,x2} and {x1,x3}.  pos[k] is the slot of row
+// x_k whose entry changes: row x0: x1 -> x2, row x1: x0 -> x3,
+// row x2: x3 -> x0, row x3: x2 -> x1.  A valid swap has 4 distinct endpoints.
+struct Swap {
+  int line[2];
+  int x[4];
+  int pos[4];
+  int valid;
+  int pad_;
+};
+
+struct State {
+  int N, d, lines, K;
+  int* edges;            // [lines][2], current graph
+  int* adj;              // [N][d], current graph
+  int* best_edges;       // [lines][2]
+  long long cur_total, best_total, prev_total;
+  int cur_diam, best_diam;
+  double temp, cooling;
+  int hill;              // 1: accept only when not worse (the reference's -H)
+  int done;              // target reached: every kernel of a step returns at once
+  int accepted;          // the last step moved the current graph
+  int n_comp;            // swaps in this step's composite
+  int best_k;            // rank-0 candidate of this step
+  int pad_;
+  long long step, accepts, multi_accepts, moved_swaps, evals, best_step, pred_accepts;
+  int n_pred;            // swaps in this step's predicted list (learned mode)
+  int pad2_;
+  long long target_total;
+  int target_diam;
+  int stop_on_target;
+  unsigned long long seed;
+  float label_scale, label_clip;
+};
+
+constexpr unsigned long long kGolden = 0x9e3779b97f4a7c15ULL;
+
+__device__ __forceinline__ unsigned long long mix64(unsigned long long z) {
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+  return z ^ (z >> 31);
+}
+
+// A counter-based stream: one 64-bit draw per (seed, a, b, c).
+__device__ __forceinline__ unsigned long long draw(unsigned long long seed, unsigned long long a, unsigned long long b,
+                                                   unsigned long long c) {
+  return mix64(seed + kGolden * (mix64(a + kGolden) ^ mix64(b * 0xd1b54a32d192ed03ULL + c + 1)));
+}
+
+__device__ __forceinline__ int below(unsigned long long h, int n) {
+  return (int)(((h >> 32) * (unsigned long long)(unsigned)n) >> 32);
+}
+
+__device__ __forceinline__ int find_in_row(const int* row, int d, int x) {
+  for (int j = 0; j < d; ++j)
+    if (row[j] == x) return j;
+  return -1;
+}
+
+// ---- gen: candidate swaps ------------------------------------------------------
+__global__ void gen_kernel(const State* __restrict__ s, Swap* __restrict__ out, int G) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= G) return;
+  Swap w;
+  w.valid = 0;
+  w.pad_ = 0;
+  if (!s->done) {
+    const int lines = s->lines, d = s->d;
+    const int* __restrict__ E = s->edges;
+    const int* __restrict__ A = s->adj;
+    const unsigned long long seed = s->seed, step = (unsigned long long)s->step;
+    for (int attempt = 0; attempt < 64 && !w.valid; ++attempt) {
+      const unsigned long long h = draw(seed, step, (unsigned long long)k, (unsigned long long)attempt);
+      const int i = below(h, lines), j = below(h << 32, lines);
+      if (i == j) continue;
+      const int r = (int)(mix64(h) & 1);
+      const int a = E[2 * i], b = E[2 * i + 1], c = E[2 * j], e = E[2 * j + 1];
+      const int x0 = a, x1 = b, x2 = r ? e : c, x3 = r ? c : e;
+      if (x0 == x2 || x1 == x3) continue;
+      const int* r0 = A + (long long)x0 * d;
+      const int* r1 = A + (long long)x1 * d;
+      if (find_in_row(r0, d, x2) >= 0 || find_in_row(r1, d, x3) >= 0) continue;
+      const int p0 = find_in_row(r0, d, x1), p1 = find_in_row(r1, d, x0);
+      const int p2 = find_in_row(A + (long long)x2 * d, d, x3), p3 = find_in_row(A + (long long)x3 * d, d, x2);
+      if (p0 < 0 || p1 < 0 || p2 < 0 || p3 < 0) continue;
+      w.line[0] = i;
+      w.line[1] = j;
+      w.x[0] = x0; w.x[1] = x1; w.x[2] = x2; w.x[3] = x3;
+      w.pos[0] = p0; w.pos[1] = p1; w.pos[2] = p2; w.pos[3] = p3;
+      w.valid = 1;
+    }
+  }
+  out[k] = w;
+}
+
+// ---- materialize: candidate adjacencies into the batch slots ---------------------
+// Slot k (blockIdx.y) = the current adjacency with candidate sel[k]'s four
+// entries changed (the current adjacency itself for an invalid candidate).
+__global__ void materialize_kernel(const State* __restrict__ s, const Swap* __restrict__ sw,
+                                   const int* __restrict__ sel, int* __restrict__ slots, long long slot_stride) {
+  if (s->done) return;
+  const int k = blockIdx.y;
+  const Swap w = sw[sel ? sel[k] : k];
+  const int d = s->d;
+  const long long n = (long long)s->N * d;
+  long long off[4] = {-1, -1, -1, -1};
+  int val[4] = {0, 0, 0, 0};
+  if (w.valid) {
+    const int nv[4] = {w.x[2], w.x[3], w.x[0], w.x[1]};
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      off[q] = (long long)w.x[q] * d + w.pos[q];
+      val[q] = nv[q];
+    }
+  }
+  const int* __restrict__ src = s->adj;
+  int* __restrict__ dst = slots + (long long)k * slot_stride;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    int v = src[i];
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+      if (i == off[q]) v = val[q];
+    dst[i] = v;
+  }
+}
+
+struct Key {
+  int diam;           // INT_MAX when disconnected or not evaluated
+  long long total;
+};
+
+__device__ __forceinline__ Key key_of(const BatchOut& o, int N) {
+  Key k;
+  if (o.done && !o.disconnected && o.diam < N) {
+    k.diam = o.diam;
+    k.total = o.sum + (long long)N * (N - 1);
+  } else {
+    k.diam = INT_MAX;
+    k.total = LLONG_MAX;
+  }
+  return k;
+}
+
+__device__ __forceinline__ bool key_less(const Key& a, const Key& b) {
+  return a.diam < b.diam || (a.diam == b.diam && a.total < b.total);
+}
+
+// ---- compose: rank the candidates, build the composite -----------------------------
+// One block of kComposeThreads threads, K <= kComposeThreads.
+constexpr int kComposeThreads = 256;
+__global__ void __launch_bounds__(kComposeThreads) compose_kernel(State* __restrict__ s, const Swap* __restrict__ sw,
+                                                                  const int* __restrict__ sel,
+                                                                  const BatchOut* __restrict__ out, int K,
+                                                                  Swap* __restrict__ comp, int compose_max,
+                                                                  unsigned* __restrict__ vmark) {
+  __shared__ int s_order[kComposeThreads];
+  if (s->done) return;
+  const int N = s->N;
+  const int k = threadIdx.x;
+  if (k < K) {
+    const Key me = key_of(out[k], N);
+    int rank = 0;
+    for (int j = 0; j < K; ++j) {
+      const Key o = key_of(out[j], N);
+      rank += key_less(o, me) || (!key_less(me, o) && j < k);
+    }
+    s_order[rank] = k;
+  }
+  __syncthreads();
+  if (k != 0) return;
+  s->prev_total = s->cur_total;
+  s->best_k = s_order[0];
+  const Key cur = {s->cur_diam, s->cur_total};
+  int m = 0;
+  for (int r = 0; r < K && m < compose_max; ++r) {
+    const int c = s_order[r];
+    const Key kc = key_of(out[c], N);
+    if (!key_less(kc, cur)) break;   // sorted: nothing further improves
+    const Swap w = sw[sel ? sel[c] : c];
+    if (!w.valid) continue;
+    bool free_ = true;
+    for (int q = 0; q < 4; ++q) free_ &= !((vmark[w.x[q] >> 5] >> (w.x[q] & 31)) & 1u);
+    if (!free_) continue;
+    for (int q = 0; q < 4; ++q) vmark[w.x[q] >> 5] |= 1u << (w.x[q] & 31);
+    comp[m++] = w;
+  }
+  for (int i = 0; i < m; ++i)
+    for (int q = 0; q < 4; ++q) vmark[comp[i].x[q] >> 5] = 0u;
+  s->n_comp = m;
+}
+
+// The composite graph: the current adjacency (copy), then its swaps.
+__global__ void copy_current_kernel(const State* __restrict__ s, int* __restrict__ dst) {
+  if (s->done) return;
+  const long long n = (long long)s->N * s->d;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    dst[i] = s->adj[i];
+}
+
+// Size of predicted composite c: the first n_pred >> c swaps of the list.
+__device__ __forceinline__ int pred_size(int n_pred, int c) { return n_pred >> c; }
+
+__device__ __forceinline__ void apply_swap(int* adj, int d, const Swap& w) {
+  adj[(long long)w.x[0] * d + w.pos[0]] = w.x[2];
+  adj[(long long)w.x[1] * d + w.pos[1]] = w.x[3];
+  adj[(long long)w.x[2] * d + w.pos[2]] = w.x[0];
+  adj[(long long)w.x[3] * d + w.pos[3]] = w.x[1];
+}
+
+__global__ void patch_composite_kernel(const State* __restrict__ s, const Swap* __restrict__ comp,
+                                       int* __restrict__ dst) {
+  if (s->done) return;
+  for (int i = threadIdx.x; i < s->n_comp; i += blockDim.x) apply_swap(dst, s->d, comp[i]);
+}
+
+// ---- decide ---------------------------------------------------------------------------
+// general/sa.c:371-411 on exact totals: with groups = 1 the reference's
+// diff = (current_ASPL - new_ASPL) * N(N-1) is the change of the distance
+// total.  Threads k < K also write the training labels of this step.
+__global__ void decide_kernel(State* __restrict__ s, const Swap* __restrict__ sw, const int* __restrict__ sel,
+                              const BatchOut* __restrict__ out, int K, const Swap* __restrict__ comp,
+                              const BatchOut* __restrict__ comp_out, float* __restrict__ labels,
+                              const Swap* __restrict__ pred, int C) {
+  if (s->done) return;
+  const int N = s->N;
+  const int k = threadIdx.x;
+  if (labels && k < K) {
+    const Key kk = key_of(out[k], N);
+    float lab = s->label_clip;
+    if (kk.diam != INT_MAX) {
+      lab = (float)((double)(kk.total - s->prev_total) * (double)s->label_scale);
+      lab = fminf(fmaxf(lab, -s->label_clip), s->label_clip);
+    }
+    labels[k] = lab;
+  }
+  if (k != 0) return;
+  const Key cur = {s->cur_diam, s->cur_total};
+  const int bk = s->best_k;
+  Key cand = key_of(out[bk], N);
+  bool use_comp = false;
+  int use_pred = 0;   // swaps of the chosen predicted composite (0: none)
+  if (comp_out && s->n_comp >= 2) {
+    const Key kc = key_of(comp_out[0], N);
+    if (key_less(kc, cand)) {
+      cand = kc;
+      use_comp = true;
+    }
+  }
+  for (int c = 0; c < C; ++c) {
+    const int m = pred_size(s->n_pred, c);
+    if (m < 1) break;
+    const Key kp = key_of(out[K + c], N);
+    if (key_less(kp, cand)) {
+      cand = kp;
+      use_comp = false;
+      use_pred = m;
+    }
+  }
+  bool acc = false;
+  if (cand.diam != INT_MAX) {
+    if (cand.diam < cur.diam) {
+      acc = true;
+    } else if (cand.diam == cur.diam) {
+      if (cand.total <= cur.total) {
+        acc = true;
+      } else if (!s->hill) {
+        const double diff = (double)(cur.total - cand.total);
+        const unsigned long long h = draw(s->seed ^ 0x5bd1e995ULL, (unsigned long long)s->step, 0x0dec1deULL, 7);
+        const double u = ((double)(h >> 11) + 1.0) / (9007199254740992.0 + 2.0);
+        acc = exp(diff / s->temp) > u;
+      }
+    }
+  }
+  s->evals += K + C + (comp_out ? 1 : 0);
+  if (acc) {
+    const int d = s->d;
+    if (use_pred) {
+      for (int i = 0; i < use_pred; ++i) {
+        const Swap& w = pred[i];
+        apply_swap(s->adj, d, w);
+        s->edges[2 * w.line[0]] = w.x[0];
+        s->edges[2 * w.line[0] + 1] = w.x[2];
+        s->edges[2 * w.line[1]] = w.x[1];
+        s->edges[2 * w.line[1] + 1] = w.x[3];
+      }
+      s->multi_accepts += 1;
+      s->pred_accepts += 1;
+      s->moved_swaps += use_pred;
+    } else if (use_comp) {
+      for (int i = 0; i < s->n_comp; ++i) {
+        const Swap& w = comp[i];
+        apply_swap(s->adj, d, w);
+        s->edges[2 * w.line[0]] = w.x[0];
+        s->edges[2 * w.line[0] + 1] = w.x[2];
+        s->edges[2 * w.line[1]] = w.x[1];
+        s->edges[2 * w.line[1] + 1] = w.x[3];
+      }
+      s->multi_accepts += 1;
+      s->moved_swaps += s->n_comp;
+    } else {
+      const Swap w = sw[sel ? sel[bk] : bk];
+      apply_swap(s->adj, d, w);
+      s->edges[2 * w.line[0]] = w.x[0];
+      s->edges[2 * w.line[0] + 1] = w.x[2];
+      s->edges[2 * w.line[1]] = w.x[1];
+      s->edges[2 * w.line[1] + 1] = w.x[3];
+      s->moved_swaps += 1;
+    }
+    s->accepts += 1;
+    s->cur_diam = cand.diam;
+    s->cur_total = cand.total;
+    if (cand.diam < s->best_diam || (cand.diam == s->best_diam && cand.total < s->best_total)) {
+      s->best_diam = cand.diam;
+      s->best_total = cand.total;
+      s->best_step = s->step;
+    }
+  }
+  s->accepted = acc ? 1 : 0;
+  if (s->stop_on_target && s->cur_diam <= s->target_diam && s->cur_total <= s->target_total) s->done = 1;
+  s->temp *= s->cooling;
+  s->step += 1;
+}
+
+// Copies the current edges to the best edges when this step set a new best.
+__global__ void best_copy_kernel(const State* __restrict__ s) {
+  if (s->best_step != s->step - 1) return;
+  const long long n = 2LL * s->lines;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    s->best_edges[i] = s->edges[i];
+}
+
+// ---- learned mode: features and selection ---------------------------------------------
+constexpr int kMaxFeatDegree = 16;
+
+// Distance between x and y resolved up to 5 (5 meaning >= 5): y in N(x),
+// N(x) meets N(y), N(x) meets N2(y), N2(x) meets N2(y), where N2(v) lists
+// the neighbours of v's neighbours (d^2 entries, kept in local memory).
+__device__ int joined_distance(const int* __restrict__ A, int d, int x, int y) {
+  if (x == y) return 0;
+  const int* rx = A + (long long)x * d;
+  const int* ry = A + (long long)y * d;
+  for (int j = 0; j < d; ++j)
+    if (rx[j] == y) return 1;
+  int n2y[kMaxFeatDegree * kMaxFeatDegree];
+  int m = 0;
+  for (int j = 0; j < d; ++j) {
+    const int* ru = A + (long long)ry[j] * d;
+    for (int q = 0; q < d; ++q) n2y[m++] = ru[q];
+  }
+  for (int i = 0; i < d; ++i)
+    for (int j = 0; j < d; ++j)
+      if (rx[i] == ry[j]) return 2;
+  for (int i = 0; i < d; ++i)
+    for (int j = 0; j < m; ++j)
+      if (rx[i] == n2y[j]) return 3;
+  for (int i = 0; i < d; ++i) {
+    const int* ru = A + (long long)rx[i] * d;
+    for (int q = 0; q < d; ++q) {
+      const int w = ru[q];
+      for (int j = 0; j < m; ++j)
+        if (w == n2y[j]) return 4;
+    }
+  }
+  return 5;
+}
+
+__device__ int capped_distance(const int* __restrict__ A, int d, int x, int y) {
+  if (x == y) return 0;
+  const int* rx = A + (long long)x * d;
+  const int* ry = A + (long long)y * d;
+  int ny[kMaxFeatDegree];
+  for (int j = 0; j < d; ++j) ny[j] = ry[j];
+  for (int j = 0; j < d; ++j)
+    if (rx[j] == y) return 1;
+  bool two = false;
+  for (int i = 0; i < d && !two; ++i) {
+    const int u = rx[i];
+    for (int j = 0; j < d; ++j) two |= (ny[j] == u);
+  }
+  if (two) return 2;
+  for (int i = 0; i < d; ++i) {
+    const int* ru = A + (long long)rx[i] * d;
+    for (int q = 0; q < d; ++q) {
+      const int w = ru[q];
+      for (int j = 0; j < d; ++j)
+        if (ny[j] == w) return 3;
+    }
+  }
+  return 4;
+}
+
+__device__ int common_neighbours(const int* __restrict__ A, int d, int x, int y) {
+  const int* rx = A + (long long)x * d;
+  const int* ry = A + (long long)y * d;
+  int c = 0;
+  for (int i = 0; i < d; ++i) {
+    const int u = rx[i];
+    for (int j = 0; j < d; ++j) c += (ry[j] == u);
+  }
+  return c;
+}
+
+// 32 features per candidate, from the current graph's profile (stats) and
+// adjacency: per endpoint (6 each) eccentricity / 8, mean distance / 8 and
+// log-scaled counts of vertices at distance 2..5; the distances of the
+// pairs the swap joins (1..4 or >= 5) and of the two cross pairs (1..3 or
+// >= 4);
+// the common-neighbour counts of the pairs it separates; and the
+// transmission gaps of the joined pairs.
+__global__ void features_kernel(const State* __restrict__ s, const Swap* __restrict__ sw, int G,
+                                const unsigned* __restrict__ stats, bf16* __restrict__ X) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= G) return;
+  float f[mlp::kFeatures];
+#pragma unroll
+  for (int i = 0; i < mlp::kFeatures; ++i) f[i] = 0.f;
+  const Swap w = sw[k];
+  if (!s->done && w.valid) {
+    const int N = s->N, d = s->d;
+    const float inv_logn = 1.f / logf(1.f + (float)N);
+    float T[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const unsigned* st = stats + (long long)w.x[e] * kStatLevels;
+      int ecc = kStatLevels - 1;
+      double tr = 0.0;
+      for (int q = 0; q < kStatLevels; ++q) {
+        tr += st[q];
+        if (st[q] == 0u && q < ecc) ecc = q;
+      }
+      T[e] = (float)tr;
+      f[6 * e + 0] = (float)ecc * 0.125f;
+      f[6 * e + 1] = (float)(tr / (double)(N - 1)) * 0.125f;
+#pragma unroll
+      for (int q = 2; q <= 5; ++q) {
+        const float nq = (float)(st[q - 1] - st[q]);
+        f[6 * e + q] = logf(1.f + nq) * inv_logn;
+      }
+    }
+    const int* A = s->adj;
+    f[24] = joined_distance(A, d, w.x[0], w.x[2]) * 0.2f;
+    f[25] = joined_distance(A, d, w.x[1], w.x[3]) * 0.2f;
+    f[26] = capped_distance(A, d, w.x[0], w.x[3]) * 0.25f;
+    f[27] = capped_distance(A, d, w.x[1], w.x[2]) * 0.25f;
+    f[28] = (float)common_neighbours(A, d, w.x[0], w.x[1]) / (float)d;
+    f[29] = (float)common_neighbours(A, d, w.x[2], w.x[3]) / (float)d;
+    f[30] = fabsf(T[0] - T[2]) / (float)(N - 1);
+    f[31] = fabsf(T[1] - T[3]) / (float)(N - 1);
+  }
+  bf16* row = X + (long long)k * mlp::kFeatures;
+#pragma unroll
+  for (int i = 0; i < mlp::kFeatures; ++i) row[i] = __float2bfloat16_rn(f[i]);
+}
+
+// Keeps the K - n_rand candidates with the smallest predicted change
+// (invalid ones last) and n_rand more drawn from the rest, and writes the
+// whole ranking (rank, rank_key) for the predicted composites.  One block of
+// 1024 threads, bitonic sort of G <= kMaxProposals (key, index) pairs.
+constexpr int kMaxProposals = 4096;
+__global__ void __launch_bounds__(1024) select_kernel(const State* __restrict__ s, const Swap* __restrict__ sw,
+                                                      const float* __restrict__ y, int G, int K, int n_rand,
+                                                      int* __restrict__ sel, int* __restrict__ rank,
+                                                      float* __restrict__ rank_key) {
+  __shared__ float s_key[kMaxProposals];
+  __shared__ int s_idx[kMaxProposals];
+  if (s->done) return;
+  int P = 1;
+  while (P < G) P <<= 1;
+  for (int i = threadIdx.x; i < P; i += blockDim.x) {
+    const bool ok = i < G && sw[i].valid;
+    s_key[i] = ok ? y[i] : FLT_MAX;
+    s_idx[i] = i < G ? i : 0;
+  }
+  __syncthreads();
+  for (int size = 2; size <= P; size <<= 1) {
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      for (int i = threadIdx.x; i < P; i += blockDim.x) {
+        const int j = i ^ stride;
+        if (j > i) {
+          const bool up = (i & size) == 0;
+          const float ki = s_key[i], kj = s_key[j];
+          const int ii = s_idx[i], ij = s_idx[j];
+          const bool gt = ki > kj || (ki == kj && ii > ij);
+          if (gt == up) {
+            s_key[i] = kj; s_key[j] = ki;
+            s_idx[i] = ij; s_idx[j] = ii;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  for (int q = threadIdx.x; q < G; q += blockDim.x) {
+    rank[q] = s_idx[q];
+    rank_key[q] = s_key[q];
+  }
+  const int top = K - n_rand;
+  for (int q = threadIdx.x; q < K; q += blockDim.x) {
+    if (q < top) {
+      sel[q] = s_idx[q];
+    } else {
+      const unsigned long long h = draw(s->seed ^ 0x243f6a8885a308d3ULL, (unsigned long long)s->step, 0x5e1ecULL, q);
+      sel[q] = s_idx[top + below(h, G - top)];
+    }
+  }
+}
+
+// The predicted list: walking the ranking best first, every valid proposal
+// predicted to lower the distance total (key < 0) whose endpoints are not
+// yet used, up to pred_max swaps.  One thread.
+__global__ void pred_list_kernel(State* __restrict__ s, const Swap* __restrict__ sw, const int* __restrict__ rank,
+                                 const float* __restrict__ rank_key, int G, int pred_max, Swap* __restrict__ pred,
+                                 unsigned* __restrict__ vmark) {
+  if (s->done || threadIdx.x != 0) return;
+  int m = 0;
+  for (int r = 0; r < G && m < pred_max; ++r) {
+    if (!(rank_key[r] < 0.f)) break;   // sorted: no further predicted gain
+    const Swap w = sw[rank[r]];
+    if (!w.valid) continue;
+    bool free_ = true;
+    for (int q = 0; q < 4; ++q) free_ &= !((vmark[w.x[q] >> 5] >> (w.x[q] & 31)) & 1u);
+    if (!free_) continue;
+    for (int q = 0; q < 4; ++q) vmark[w.x[q] >> 5] |= 1u << (w.x[q] & 31);
+    pred[m++] = w;
+  }
+  for (int i = 0; i < m; ++i)
+    for (int q = 0; q < 4; ++q) vmark[pred[i].x[q] >> 5] = 0u;
+  s->n_pred = m;
+}
+
+// Slots K .. K+C-1: the current adjacency (blockIdx.y = composite), then
+// patch_pred_kernel applies each composite's swaps.
+__global__ void copy_pred_kernel(const State* __restrict__ s, int* __restrict__ slots, long long slot_stride, int K) {
+  if (s->done) return;
+  const long long n = (long long)s->N * s->d;
+  int* dst = slots + (long long)(K + blockIdx.y) * slot_stride;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    dst[i] = s->adj[i];
+}
+
+__global__ void patch_pred_kernel(const State* __restrict__ s, const Swap* __restrict__ pred, int* __restrict__ slots,
+                                  long long slot_stride, int K) {
+  if (s->done) return;
+  const int c = blockIdx.x;
+  int* dst = slots + (long long)(K + c) * slot_stride;
+  const int m = pred_size(s->n_pred, c);
+  for (int i = threadIdx.x; i < m; i += blockDim.x) apply_swap(dst, s->d, pred[i]);
+}
+
+}  // namespace sa
+}  // namespace ggb
+
+using ggb::sa::State;
+using ggb::sa::Swap;
+
+struct ggb_sa {
+  int device = -1;
+  int sms = 0;
+  int N = 0, d = 0, lines = 0;
+  int K = 0, G = 0, n_rand = 0, compose_max = 0;
+  int C = 0, pred_max = 0;        // predicted composites (learned mode) and their largest size
+  bool learned = false;
+  State h{};                      // host mirror of the device state
+  State* d_state = nullptr;
+  int* d_edges = nullptr;
+  int* d_adj = nullptr;
+  int* d_best_edges = nullptr;
+  Swap* d_swaps = nullptr;        // [G]
+  int* d_sel = nullptr;           // [K]
+  Swap* d_comp = nullptr;         // [compose_max]
+  unsigned* d_vmark = nullptr;    // [N/32 + 1]
+  float* d_labels = nullptr;      // [K]
+  float* d_scores = nullptr;      // [G]
+  __nv_bfloat16* d_X = nullptr;   // [G][32]
+  unsigned* d_stats = nullptr;    // [N][kStatLevels]
+  int* d_sticky = nullptr;        // first device error of any evaluation in a step
+  ggb_batch* cand = nullptr;      // K candidates, then C predicted composites
+  int* d_rank = nullptr;          // [G] ranking of the proposals
+  float* d_rank_key = nullptr;    // [G]
+  Swap* d_pred = nullptr;         // [pred_max]
+  ggb_batch* comp = nullptr;      // the composite
+  ggb_mlp* mlp = nullptr;
+  // profile launch
+  int pR = 0;
+  ggb::ApspCtrl* d_pctrl = nullptr;
+  uint4* d_pbuf = nullptr;
+  cudaStream_t st = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+
+namespace {
+
+template <typename T>
+int sdev(T** p, size_t n) {
+  if (cudaMalloc(p, std::max<size_t>(n, 1) * sizeof(T)) != cudaSuccess) {
+    cudaGetLastError();
+    *p = nullptr;
+    return core_fail(GGB_ENOMEM, "cudaMalloc of %zu bytes failed", n * sizeof(T));
+  }
+  return GGB_OK;
+}
+
+const void* profile_kernel_for(int R) {
+  switch (R) {
+    case 16: return (const void*)ggb::apsp_profile_kernel<16>;
+    case 32: return (const void*)ggb::apsp_profile_kernel<32>;
+    case 64: return (const void*)ggb::apsp_profile_kernel<64>;
+    default: return nullptr;
+  }
+}
+
+size_t profile_smem_for(int R) {
+  switch (R) {
+    case 16: return ggb::apsp_smem_bytes<16>();
+    case 32: return ggb::apsp_smem_bytes<32>();
+    case 64: return ggb::apsp_smem_bytes<64>();
+    default: return 0;
+  }
+}
+
+int enqueue_profile(ggb_sa* a, const int* gate, cudaStream_t st) {
+  SCUDA(cudaMemsetAsync(a->d_pctrl, 0, sizeof(ggb::ApspCtrl), st));
+  ggb::ApspArgs p;
+  std::memset(&p, 0, sizeof p);
+  p.adj = a->d_adj;
+  p.adj2 = nullptr;
+  p.buf0 = a->d_pbuf;
+  p.buf1 = a->d_pbuf + (size_t)a->N * a->pR;
+  p.ctrl = a->d_pctrl;
+  p.timeout_ns = 2000000000LL;
+  p.N = a->N;
+  p.d = a->d;
+  p.n_src1 = a->N;
+  p.split = a->N;
+  p.ac = 0;
+  p.groups = 1;
+  p.win_first = 0;
+  p.win_stride = 1;
+  p.vec4 = (a->d % 4 == 0) ? 1 : 0;
+  p.stats = a->d_stats;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(a->sms);
+  cfg.blockDim = dim3(ggb::kThreads);
+  cfg.dynamicSmemBytes = profile_smem_for(a->pR);
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  int* sticky = a->d_sticky;
+  void* params[] = {(void*)&p, (void*)&gate, (void*)&sticky};
+  SCUDA(cudaLaunchKernelExC(&cfg, profile_kernel_for(a->pR), params));
+  ggb::core_add_launches(1);
+  return GGB_OK;
+}
+
+// Every kernel of one step, in order, on `st` (captured once).
+int enqueue_step(ggb_sa* a, cudaStream_t st) {
+  using namespace ggb::sa;
+  State* s = a->d_state;
+  const int G = a->learned ? a->G : a->K;
+  gen_kernel<<<(G + 127) / 128, 128, 0, st>>>(s, a->d_swaps, G);
+  int launches = 1;
+  const int* sel = nullptr;
+  if (a->learned) {
+    features_kernel<<<(G + 127) / 128, 128, 0, st>>>(s, a->d_swaps, G, a->d_stats, a->d_X);
+    int rc = ggb::mlp_forward(a->mlp, a->d_X, G, a->d_scores, st, false);
+    if (rc) return rc;
+    select_kernel<<<1, 1024, 0, st>>>(s, a->d_swaps, a->d_scores, G, a->K, a->n_rand, a->d_sel, a->d_rank,
+                                      a->d_rank_key);
+    sel = a->d_sel;
+    launches += 2;
+  }
+  const long long stride = a->cand->off.size() > 1 ? a->cand->off[1] - a->cand->off[0] : 0;
+  const int bx = std::max(1, std::min(a->sms * 4 / std::max(a->K, 1), (int)(((long long)a->N * a->d + 255) / 256)));
+  materialize_kernel<<<dim3(bx, a->K), 256, 0, st>>>(s, a->d_swaps, sel, a->cand->d_adj, stride);
+  if (a->C > 0) {
+    pred_list_kernel<<<1, 32, 0, st>>>(s, a->d_swaps, a->d_rank, a->d_rank_key, G, a->pred_max, a->d_pred,
+                                       a->d_vmark);
+    copy_pred_kernel<<<dim3(bx, a->C), 256, 0, st>>>(s, a->cand->d_adj, stride, a->K);
+    patch_pred_kernel<<<a->C, 128, 0, st>>>(s, a->d_pred, a->cand->d_adj, stride, a->K);
+    launches += 3;
+  }
+  int rc = ggb::batch_enqueue(a->cand, st);
+  if (rc) return rc;
+  compose_kernel<<<1, kComposeThreads, 0, st>>>(s, a->d_swaps, sel, a->cand->d_out, a->K, a->d_comp,
+                                                a->compose_max, a->d_vmark);
+  launches += 3;
+  const ggb::BatchOut* comp_out = nullptr;
+  if (a->compose_max >= 2) {
+    copy_current_kernel<<<a->sms, 256, 0, st>>>(s, a->comp->d_adj);
+    patch_composite_kernel<<<1, 128, 0, st>>>(s, a->d_comp, a->comp->d_adj);
+    rc = ggb::batch_enqueue(a->comp, st);
+    if (rc) return rc;
+    comp_out = a->comp->d_out;
+    launches += 3;
+  }
+  decide_kernel<<<1, std::max(32, (a->K + 31) / 32 * 32), 0, st>>>(s, a->d_swaps, sel, a->cand->d_out, a->K,
+                                                                   a->d_comp, comp_out,
+                                                                   a->learned ? a->d_labels : nullptr, a->d_pred,
+                                                                   a->C);
+  launches += 1;
+  if (a->learned) {
+    rc = ggb::mlp_train_rows(a->mlp, a->d_X, a->d_sel, a->d_labels, a->K, st);
+    if (rc) return rc;
+    rc = enqueue_profile(a, &s->accepted, st);
+    if (rc) return rc;
+  }
+  best_copy_kernel<<<a->sms, 256, 0, st>>>(s);
+  launches += 1;
+  ggb::core_add_launches(launches);
+  SCUDA(cudaGetLastError());
+  return GGB_OK;
+}
+
+int capture_step(ggb_sa* a) {
+  if (a->exec) return GGB_OK;
+  SCUDA(cudaStreamBeginCapture(a->st, cudaStreamCaptureModeThreadLocal));
+  int rc = enqueue_step(a, a->st);
+  cudaGraph_t gph = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(a->st, &gph);
+  if (rc) {
+    if (gph) cudaGraphDestroy(gph);
+    return rc;
+  }
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return core_fail(GGB_ECUDA, "capturing the annealing step failed: %s", cudaGetErrorString(e));
+  }
+  a->graph = gph;
+  SCUDA(cudaGraphInstantiate(&a->exec, gph, 0));
+  return GGB_OK;
+}
+
+int pull_state(ggb_sa* a) {
+  SCUDA(cudaMemcpyAsync(&a->h, a->d_state, sizeof(State), cudaMemcpyDeviceToHost, a->st));
+  SCUDA(cudaStreamSynchronize(a->st));
+  return GGB_OK;
+}
+
+int push_state(ggb_sa* a) {
+  SCUDA(cudaMemcpyAsync(a->d_state, &a->h, sizeof(State), cudaMemcpyHostToDevice, a->st));
+  SCUDA(cudaStreamSynchronize(a->st));
+  return GGB_OK;
+}
+
+void destroy(ggb_sa* a) {
+  if (!a) return;
+  if (a->device >= 0) cudaSetDevice(a->device);
+  if (a->st) cudaStreamSynchronize(a->st);
+  if (a->exec) cudaGraphExecDestroy(a->exec);
+  if (a->graph) cudaGraphDestroy(a->graph);
+  for (void* q : {(void*)a->d_state, (void*)a->d_edges, (void*)a->d_adj, (void*)a->d_best_edges, (void*)a->d_swaps,
+                  (void*)a->d_sel, (void*)a->d_comp, (void*)a->d_vmark, (void*)a->d_labels, (void*)a->d_scores,
+                  (void*)a->d_X, (void*)a->d_stats, (void*)a->d_pctrl, (void*)a->d_pbuf, (void*)a->d_sticky,
+                  (void*)a->d_rank, (void*)a->d_rank_key, (void*)a->d_pred})
+    cudaFree(q);
+  if (a->cand) ggb_batch_destroy(a->cand);
+  if (a->comp) ggb_batch_destroy(a->comp);
+  if (a->mlp) ggb_mlp_destroy(a->mlp);
+  if (a->st) cudaStreamDestroy(a->st);
+  cudaGetLastError();
+  delete a;
+}
+
+// Evaluates the current graph exactly (profile kernel, ungated) and sets the
+// current and best values from it.
+int evaluate_current(ggb_sa* a) {
+  int rc = enqueue_profile(a, nullptr, a->st);
+  if (rc) return rc;
+  ggb::ApspCtrl c;
+  SCUDA(cudaMemcpyAsync(&c, a->d_pctrl, sizeof c, cudaMemcpyDeviceToHost, a->st));
+  SCUDA(cudaStreamSynchronize(a->st));
+  if (c.error == ggb::kErrAdj) return core_fail(GGB_EADJ, "edge list has an endpoint outside [0, nodes)");
+  if (c.error) return core_fail(GGB_ECUDA, "profile evaluation failed (device error %d)", c.error);
+  if (!c.done) return core_fail(GGB_ECUDA, "profile evaluation did not complete");
+  if (c.disconnected || c.diam >= a->N) return core_fail(GGB_EINVAL, "the initial graph is not connected");
+  a->h.cur_diam = a->h.best_diam = c.diam;
+  a->h.cur_total = a->h.best_total = a->h.prev_total = c.sum + (long long)a->N * (a->N - 1);
+  return GGB_OK;
+}
+
+int create(ggb_sa* a, int nodes, int degree, const int* edges, int K, int G, int compose_max,
+           unsigned long long seed) {
+  using namespace ggb::sa;
+  a->N = nodes;
+  a->d = degree;
+  a->lines = (int)((long long)nodes * degree / 2);
+  a->K = K;
+  a->G = G;
+  a->learned = G > K;
+  a->compose_max = compose_max;
+  a->n_rand = a->learned ? std::max(1, K / 4) : 0;
+  a->C = a->learned ? 4 : 0;
+  a->pred_max = a->learned ? 64 : 0;
+  int dev = 0;
+  SCUDA(cudaGetDevice(&dev));
+  a->device = dev;
+  SCUDA(cudaDeviceGetAttribute(&a->sms, cudaDevAttrMultiProcessorCount, dev));
+  int l2 = 0;
+  SCUDA(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, dev));
+  SCUDA(cudaStreamCreateWithFlags(&a->st, cudaStreamNonBlocking));
+  // edges -> adjacency (general/sa.c:61-74 order), with the checks of a simple regular graph
+  std::vector<int> adj((size_t)nodes * degree), fill(nodes, 0);
+  for (int i = 0; i < a->lines; ++i) {
+    const int u = edges[2 * i], v = edges[2 * i + 1];
+    if (u < 0 || u >= nodes || v < 0 || v >= nodes || u == v)
+      return core_fail(GGB_EINVAL, "line %d: bad endpoint or self-loop", i);
+    if (fill[u] >= degree || fill[v] >= degree) return core_fail(GGB_EINVAL, "the graph is not %d-regular", degree);
+    for (int j = 0; j < fill[u]; ++j)
+      if (adj[(size_t)u * degree + j] == v) return core_fail(GGB_EINVAL, "line %d repeats an edge", i);
+    adj[(size_t)u * degree + fill[u]++] = v;
+    adj[(size_t)v * degree + fill[v]++] = u;
+  }
+  int rc;
+  const size_t L2 = (size_t)2 * a->lines;
+  if ((rc = sdev(&a->d_state, 1)) || (rc = sdev(&a->d_edges, L2)) || (rc = sdev(&a->d_adj, adj.size())) ||
+      (rc = sdev(&a->d_best_edges, L2)) || (rc = sdev(&a->d_swaps, (size_t)std::max(G, K))) ||
+      (rc = sdev(&a->d_sel, (size_t)K)) || (rc = sdev(&a->d_comp, (size_t)std::max(compose_max, 1))) ||
+      (rc = sdev(&a->d_vmark, (size_t)nodes / 32 + 1)) || (rc = sdev(&a->d_labels, (size_t)K)) ||
+      (rc = sdev(&a->d_scores, (size_t)std::max(G, K))) ||
+      (rc = sdev(&a->d_X, (size_t)std::max(G, K) * ggb::mlp::kFeatures)) ||
+      (rc = sdev(&a->d_stats, (size_t)nodes * ggb::kStatLevels)) || (rc = sdev(&a->d_pctrl, 1)) ||
+      (rc = sdev(&a->d_sticky, 1)) || (rc = sdev(&a->d_rank, (size_t)std::max(G, K))) ||
+      (rc = sdev(&a->d_rank_key, (size_t)std::max(G, K))) || (rc = sdev(&a->d_pred, (size_t)std::max(a->pred_max, 1))))
+    return rc;
+  SCUDA(cudaMemset(a->d_sticky, 0, sizeof(int)));
+  SCUDA(cudaMemcpy(a->d_edges, edges, L2 * sizeof(int), cudaMemcpyHostToDevice));
+  SCUDA(cudaMemcpy(a->d_best_edges, edges, L2 * sizeof(int), cudaMemcpyHostToDevice));
+  SCUDA(cudaMemcpy(a->d_adj, adj.data(), adj.size() * sizeof(int), cudaMemcpyHostToDevice));
+  SCUDA(cudaMemset(a->d_vmark, 0, ((size_t)nodes / 32 + 1) * sizeof(unsigned)));
+  SCUDA(cudaMemset(a->d_swaps, 0, (size_t)std::max(G, K) * sizeof(Swap)));
+  SCUDA(cudaMemset(a->d_X, 0, (size_t)std::max(G, K) * ggb::mlp::kFeatures * sizeof(__nv_bfloat16)));
+  // profile window: the widest of 2048 / 4096 / 8192 sources whose two matrices fit in about half the L2
+  a->pR = 16;
+  for (int R = 64; R >= 16; R /= 2)
+    if ((double)2 * nodes * 16.0 * R <= 0.55 * l2) { a->pR = R; break; }
+  for (int R = 16; R <= 64; R *= 2) {
+    int nb = 0;
+    SCUDA(cudaFuncSetAttribute(profile_kernel_for(R), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)profile_smem_for(R)));
+    SCUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, profile_kernel_for(R), ggb::kThreads,
+                                                        profile_smem_for(R)));
+    if (nb < 1) return core_fail(GGB_ECUDA, "profile kernel R=%d cannot be resident", R);
+  }
+  if ((rc = sdev(&a->d_pbuf, (size_t)2 * nodes * a->pR))) return rc;
+  // the candidate batch and the composite
+  const int nb = K + a->C;
+  std::vector<int> nn(nb, nodes), bn(nb, nodes), gg(nb, 1), dd(nb, degree);
+  if ((rc = ggb_batch_create(nb, nn.data(), bn.data(), gg.data(), dd.data(), &a->cand))) return rc;
+  a->cand->stop = &a->d_state->done;
+  a->cand->sticky = a->d_sticky;
+  if (compose_max >= 2) {
+    if ((rc = ggb_batch_create(1, nn.data(), bn.data(), gg.data(), dd.data(), &a->comp))) return rc;
+    a->comp->stop = &a->d_state->done;
+    a->comp->sticky = a->d_sticky;
+    if ((rc = ggb_batch_set_plan(a->comp, 0, a->sms))) return rc;
+  }
+  if (a->learned) {
+    if ((rc = ggb_mlp_create(std::max(G, K), seed ^ 0x4d4c50ULL, &a->mlp))) return rc;
+  }
+  // initial state
+  std::memset(&a->h, 0, sizeof a->h);
+  a->h.N = nodes;
+  a->h.d = degree;
+  a->h.lines = a->lines;
+  a->h.K = K;
+  a->h.edges = a->d_edges;
+  a->h.adj = a->d_adj;
+  a->h.best_edges = a->d_best_edges;
+  a->h.temp = 0.0;
+  a->h.cooling = 1.0;
+  a->h.hill = 1;
+  a->h.seed = seed;
+  a->h.best_step = -1;
+  a->h.target_diam = INT_MAX;
+  a->h.target_total = LLONG_MIN;
+  a->h.label_scale = 16.0f / (float)nodes;
+  a->h.label_clip = 16.0f;
+  if ((rc = push_state(a))) return rc;
+  if ((rc = evaluate_current(a))) return rc;
+  if ((rc = push_state(a))) return rc;
+  // candidate slots hold the current graph until the first step
+  for (int k = 0; k < nb; ++k) {
+    int* slot = nullptr;
+    ggb_batch_adj_device(a->cand, k, &slot);
+    SCUDA(cudaMemcpy(slot, a->d_adj, adj.size() * sizeof(int), cudaMemcpyDeviceToDevice));
+  }
+  if (a->comp) {
+    int* cslot = nullptr;
+    ggb_batch_adj_device(a->comp, 0, &cslot);
+    SCUDA(cudaMemcpy(cslot, a->d_adj, adj.size() * sizeof(int), cudaMemcpyDeviceToDevice));
+  }
+  return GGB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ggb_sa_create(int nodes, int degree, const int* edges, int candidates, int proposals, int compose_max,
+                  unsigned long long seed, ggb_sa** out) {
+  if (!out || !edges) return core_fail(GGB_EINVAL, "null pointer");
+  *out = nullptr;
+  if (nodes < 4 || degree < 1 || ((long long)nodes * degree) % 2 || (long long)nodes * degree > INT_MAX)
+    return core_fail(GGB_EINVAL, "nodes >= 4, degree >= 1 and nodes*degree even are required");
+  if (candidates < 1 || candidates > ggb::sa::kComposeThreads)
+    return core_fail(GGB_EINVAL, "candidates must be in [1, %d]", ggb::sa::kComposeThreads);
+  if (proposals < candidates) proposals = candidates;
+  if (proposals > candidates) {
+    if (proposals > ggb::sa::kMaxProposals || proposals % 16)
+      return core_fail(GGB_EINVAL, "proposals must be a multiple of 16 up to %d", ggb::sa::kMaxProposals);
+    if (candidates % 16 || candidates > ggb::mlp::kMaxTrainRows)
+      return core_fail(GGB_EINVAL, "with a proposal filter, candidates must be a multiple of 16 up to %d",
+                       ggb::mlp::kMaxTrainRows);
+    if (degree > ggb::sa::kMaxFeatDegree)
+      return core_fail(GGB_EINVAL, "the proposal filter's features support degree <= %d", ggb::sa::kMaxFeatDegree);
+  }
+  if (compose_max < 0 || compose_max > 4096) return core_fail(GGB_EINVAL, "compose_max must be in [0, 4096]");
+  ggb_sa* a = new ggb_sa();
+  int rc = create(a, nodes, degree, edges, candidates, proposals, compose_max, seed);
+  if (rc) {
+    destroy(a);
+    return rc;
+  }
+  *out = a;
+  return GGB_OK;
+}
+
+void ggb_sa_destroy(ggb_sa* a) { destroy(a); }
+
+int ggb_sa_set_schedule(ggb_sa* a, double temp, double cooling_rate, int hill_climbing) {
+  if (!a) return core_fail(GGB_EINVAL, "null annealer");
+  if (!(temp >= 0.0) || !(cooling_rate > 0.0)) return core_fail(GGB_EINVAL, "temp >= 0 and cooling_rate > 0");
+  if (!hill_climbing && !(temp > 0.0)) return core_fail(GGB_EINVAL, "annealing needs temp > 0");
+  SCUDA(cudaSetDevice(a->device));
+  int rc = pull_state(a);
+  if (rc) return rc;
+  a->h.temp = temp;
+  a->h.cooling = cooling_rate;
+  a->h.hill = hill_climbing ? 1 : 0;
+  return push_state(a);
+}
+
+int ggb_sa_set_target(ggb_sa* a, int diameter, long long total) {
+  if (!a) return core_fail(GGB_EINVAL, "null annealer");
+  SCUDA(cudaSetDevice(a->device));
+  int rc = pull_state(a);
+  if (rc) return rc;
+  a->h.stop_on_target = 1;
+  a->h.target_diam = diameter;
+  a->h.target_total = total;
+  a->h.done = (a->h.cur_diam <= diameter && a->h.cur_total <= total) ? 1 : 0;
+  return push_state(a);
+}
+
+int ggb_sa_autotune(ggb_sa* a, int iters, int* window_bits, int* team_ctas, double* best_ms) {
+  if (!a) return core_fail(GGB_EINVAL, "null annealer");
+  SCUDA(cudaSetDevice(a->device));
+  if (a->exec) {
+    cudaGraphExecDestroy(a->exec);
+    cudaGraphDestroy(a->graph);
+    a->exec = nullptr;
+    a->graph = nullptr;
+  }
+  return ggb_batch_autotune(a->cand, iters, window_bits, team_ctas, best_ms);
+}
+
+int ggb_sa_run(ggb_sa* a, long long steps, ggb_sa_stats* stats) {
+  if (!a || steps < 0) return core_fail(GGB_EINVAL, "null annealer or negative steps");
+  SCUDA(cudaSetDevice(a->device));
+  int rc = capture_step(a);
+  if (rc) return rc;
+  for (long long i = 0; i < steps; ++i) SCUDA(cudaGraphLaunch(a->exec, a->st));
+  SCUDA(cudaStreamSynchronize(a->st));
+  int sticky = 0;
+  SCUDA(cudaMemcpy(&sticky, a->d_sticky, sizeof sticky, cudaMemcpyDeviceToHost));
+  if (sticky == ggb::kErrTimeout) return core_fail(GGB_ETIMEOUT, "a barrier wait of an annealing step ran out");
+  if (sticky == ggb::kErrAdj) return core_fail(GGB_EADJ, "an annealing candidate had an entry outside [0, nodes)");
+  if (sticky) return core_fail(GGB_ECUDA, "an annealing evaluation failed (device error %d)", sticky);
+  rc = pull_state(a);
+  if (rc) return rc;
+  if (stats) {
+    const double pairs = (double)a->N * (a->N - 1);
+    stats->step = a->h.step;
+    stats->accepts = a->h.accepts;
+    stats->multi_accepts = a->h.multi_accepts;
+    stats->moved_swaps = a->h.moved_swaps;
+    stats->pred_accepts = a->h.pred_accepts;
+    stats->evals = a->h.evals;
+    stats->cur_diam = a->h.cur_diam;
+    stats->best_diam = a->h.best_diam;
+    stats->cur_total = a->h.cur_total;
+    stats->best_total = a->h.best_total;
+    stats->cur_aspl = (double)a->h.cur_total / pairs;
+    stats->best_aspl = (double)a->h.best_total / pairs;
+    stats->temp = a->h.temp;
+    stats->done = a->h.done;
+  }
+  return GGB_OK;
+}
+
+int ggb_sa_edges(ggb_sa* a, int best, int* edges) {
+  if (!a || !edges) return core_fail(GGB_EINVAL, "null pointer");
+  SCUDA(cudaSetDevice(a->device));
+  SCUDA(cudaStreamSynchronize(a->st));
+  SCUDA(cudaMemcpy(edges, best ? a->d_best_edges : a->d_edges, (size_t)2 * a->lines * sizeof(int),
+                   cudaMemcpyDeviceToHost));
+  return GGB_OK;
+}
+
+int ggb_sa_last_step(ggb_sa* a, float* predicted, float* label) {
+  if (!a || !predicted || !label) return core_fail(GGB_EINVAL, "null pointer");
+  if (!a->learned) return core_fail(GGB_EPERM, "the annealer has no proposal filter");
+  SCUDA(cudaSetDevice(a->device));
+  SCUDA(cudaStreamSynchronize(a->st));
+  std::vector<int> sel(a->K);
+  std::vector<float> sc(a->G);
+  SCUDA(cudaMemcpy(sel.data(), a->d_sel, a->K * sizeof(int), cudaMemcpyDeviceToHost));
+  SCUDA(cudaMemcpy(sc.data(), a->d_scores, a->G * sizeof(float), cudaMemcpyDeviceToHost));
+  SCUDA(cudaMemcpy(label, a->d_labels, a->K * sizeof(float), cudaMemcpyDeviceToHost));
+  for (int k = 0; k < a->K; ++k) predicted[k] = sc[sel[k]];
+  return GGB_OK;
+}
+
+int ggb_sa_profile(ggb_sa* a, unsigned* stats) {
+  if (!a || !stats) return core_fail(GGB_EINVAL, "null pointer");
+  SCUDA(cudaSetDevice(a->device));
+  int rc = enqueue_profile(a, nullptr, a->st);
+  if (rc) return rc;
+  SCUDA(cudaStreamSynchronize(a->st));
+  SCUDA(cudaMemcpy(stats, a->d_stats, (size_t)a->N * ggb::kStatLevels * sizeof(unsigned), cudaMemcpyDeviceToHost));
+  return GGB_OK;
+}
+
+}  // extern "C"

@@ -279,6 +279,89 @@ int ggb_batch_eval(ggb_batch *b, const int *const *adj, ggb_result *results);
 /* Device time of the last collected launch (CUDA events around it). */
 int ggb_batch_kernel_ms(const ggb_batch *b, double *ms);
 
+/* ---- the proposal filter's network (learned annealing) ------------------ */
+
+/* A 32 -> 256 -> 256 -> 1 ReLU MLP on BF16 tensor cores with FP32
+ * accumulation, trained with Adam on the mean squared error.  The annealing
+ * engine (ggb_sa_*) owns one; these entry points exist so the network can be
+ * checked on its own (host arrays in and out).  Parameters are packed FP32:
+ * W1 [256][32], b1 [256], W2 [256][256], b2 [256], w3 [256], b3 [1]
+ * (ggb_mlp_param_count() values).  No counterpart in the reference. */
+typedef struct ggb_mlp ggb_mlp;
+int ggb_mlp_create(int max_rows, unsigned long long seed, ggb_mlp **out);
+void ggb_mlp_destroy(ggb_mlp *m);
+int ggb_mlp_param_count(void);
+int ggb_mlp_set_params(ggb_mlp *m, const float *params);   /* also resets Adam */
+int ggb_mlp_get_params(ggb_mlp *m, float *params);
+int ggb_mlp_set_adam(ggb_mlp *m, float lr, float beta1, float beta2, float eps);
+/* y[r] for rows x 32 FP32 features (rounded to BF16 on the way in);
+ * rows % 16 == 0, rows <= max_rows. */
+int ggb_mlp_forward_host(ggb_mlp *m, const float *x, int rows, float *y);
+/* Loss and gradients (packed like the parameters) of the mean squared error
+ * of rows samples against targets t; rows % 16 == 0, rows <= 256. */
+int ggb_mlp_grads_host(ggb_mlp *m, const float *x, const float *t, int rows, float *loss, float *grads);
+/* `steps` Adam steps on the same rows; reports the loss of the last one. */
+int ggb_mlp_train_host(ggb_mlp *m, const float *x, const float *t, int rows, int steps, float *last_loss);
+
+/* ---- annealing on the device -------------------------------------------- */
+
+/* Simulated annealing of a simple degree-regular general graph (groups = 1,
+ * no added centres) with the whole step on the device, replayed as one CUDA
+ * graph per step.  Each step draws `proposals` 2-opt swaps of the current
+ * graph (general/sa.c:217-369 rules: no self-loop, no repeated edge); when
+ * proposals > candidates, the proposal filter's network ranks them and the
+ * best `candidates` (a quarter of them drawn at random from the rest) are
+ * evaluated exactly in one batch launch, together with four predicted
+ * composites: the first m, m/2, m/4, m/8 proposals of the ranking that are
+ * predicted to help and have disjoint endpoints, each applied to the current
+ * graph as one move.  The strictly improving candidates with disjoint
+ * endpoints (at most compose_max) are composed into one more graph, evaluated
+ * exactly too; the best of all these exactly evaluated graphs is accepted by
+ * the reference's rule (general/sa.c:371-411: smaller diameter,
+ * or equal diameter and a distance total not larger, or, when not
+ * hill-climbing, exp(diff / temp) > uniform).  With a filter, every step
+ * trains the network on the evaluated candidates' exact changes and an
+ * accepted move re-profiles the current graph.  candidates = proposals = 1,
+ * compose_max = 0 is the reference's plain step.  No host round trip per
+ * step; no counterpart for the batching and the filter in the reference. */
+typedef struct ggb_sa ggb_sa;
+
+typedef struct ggb_sa_stats {
+  long long step, accepts, multi_accepts, moved_swaps, evals;
+  long long pred_accepts;            /* accepted predicted composites */
+  int cur_diam, best_diam;
+  long long cur_total, best_total;   /* exact distance totals (the reference's sum) */
+  double cur_aspl, best_aspl;
+  double temp;
+  int done;                          /* the target was reached */
+} ggb_sa_stats;
+
+/* edges: [nodes*degree/2][2] (a simple degree-regular graph, connected).
+ * candidates in [1, 256]; proposals = candidates (no filter) or a multiple of
+ * 16 up to 4096 (then candidates is a multiple of 16, degree <= 16). */
+int ggb_sa_create(int nodes, int degree, const int *edges, int candidates, int proposals, int compose_max,
+                  unsigned long long seed, ggb_sa **out);
+void ggb_sa_destroy(ggb_sa *a);
+/* Temperature, cooling factor per step, and hill climbing (the reference's
+ * -H: accept only when not worse).  Default: hill climbing. */
+int ggb_sa_set_schedule(ggb_sa *a, double temp, double cooling_rate, int hill_climbing);
+/* Stop (every later step does nothing) once diameter <= diameter and the
+ * distance total <= total. */
+int ggb_sa_set_target(ggb_sa *a, int diameter, long long total);
+/* Autotunes the plan of the candidate batch on the current graph. */
+int ggb_sa_autotune(ggb_sa *a, int iters, int *window_bits, int *team_ctas, double *best_ms);
+/* Runs `steps` steps and reports the state. */
+int ggb_sa_run(ggb_sa *a, long long steps, ggb_sa_stats *stats);
+/* Current (best = 0) or best (best = 1) edge list, [lines][2]. */
+int ggb_sa_edges(ggb_sa *a, int best, int *edges);
+/* With a proposal filter: the network's predictions and the exact labels
+ * (scaled change of the distance total) of the last step's `candidates`
+ * evaluated swaps; the last quarter of them were drawn at random. */
+int ggb_sa_last_step(ggb_sa *a, float *predicted, float *label);
+/* Per-vertex level statistics of the current graph, [nodes][32]: entry
+ * [v][k] = vertices not within distance k of v. */
+int ggb_sa_profile(ggb_sa *a, unsigned *stats);
+
 #ifdef __cplusplus
 }
 #endif

@@ -255,3 +255,29 @@ def ref_grid_nr(adj, degs, rotate_hash, groups=1, based_nodes=None):
                         False, rh.ctypes.data)
     return bool(ok), dm.value, (asp.value if ok else None)
 
+
+
+def level_stats(adj, levels: int = 32) -> np.ndarray:
+    """[n][levels]: entry [v][k] = vertices not within distance k of v, by a
+    plain BFS from every vertex (the per-vertex statistics the profile
+    kernel accumulates; unreachable vertices count at every level)."""
+    a = np.asarray(adj)
+    n = a.shape[0]
+    out = np.zeros((n, levels), dtype=np.int64)
+    for s in range(n):
+        dist = np.full(n, -1, dtype=np.int64)
+        dist[s] = 0
+        frontier = [s]
+        k = 0
+        while frontier:
+            k += 1
+            nxt = []
+            for u in frontier:
+                for w in a[u]:
+                    if dist[w] < 0:
+                        dist[w] = k
+                        nxt.append(int(w))
+            frontier = nxt
+        for q in range(levels):
+            out[s, q] = int(np.sum((dist < 0) | (dist > q)))
+    return out

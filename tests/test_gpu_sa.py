@@ -1,0 +1,126 @@
+"""Device annealing: every reported state is the exact evaluation of the
+graph the device holds, and the graph stays simple and regular."""
+import numpy as np
+import pytest
+
+import graphgolf_b200 as gg
+import oracle
+from graphgolf_b200 import graphs
+
+pytestmark = pytest.mark.gpu
+
+
+def _exact(g, edges):
+    adj = graphs.create_adj(g.nodes, g.degree, edges)
+    h = graphs.Graph(g.nodes, g.degree, edges, adj)
+    assert graphs.verify(h) == 0
+    r = gg.evaluate(adj)
+    return r.diameter, r.total
+
+
+def _check(an, g, st):
+    assert _exact(g, an.edges()) == (st.cur_diam, st.cur_total)
+    assert _exact(g, an.edges(best=True)) == (st.best_diam, st.best_total)
+
+
+@pytest.mark.parametrize("K,G,comp", [(1, 1, 0), (8, 8, 0), (16, 16, 8), (32, 256, 16)])
+def test_hill_climbing_states_exact(gpu, K, G, comp):
+    g = graphs.random_regular(512, 6, 11)
+    with gg.Annealer(g, candidates=K, proposals=G, compose=comp, seed=3) as an:
+        st0 = an.run(0)
+        assert (st0.cur_diam, st0.cur_total) == _exact(g, g.edges)
+        prev = st0.cur_total
+        for _ in range(3):
+            st = an.run(10)
+            assert st.cur_total <= prev and st.cur_total == st.best_total
+            prev = st.cur_total
+            _check(an, g, st)
+        assert st.step == 30 and st.evals >= 30 * K
+        if comp:
+            assert st.moved_swaps >= st.accepts
+        assert st.cur_total < st0.cur_total
+
+
+def test_metropolis_states_exact(gpu):
+    g = graphs.random_regular(400, 5, 4)
+    with gg.Annealer(g, candidates=4, seed=9) as an:
+        an.schedule(temp=200.0, cooling=0.98, hill_climbing=False)
+        st = an.run(60)
+        assert st.step == 60 and abs(st.temp - 200.0 * 0.98 ** 60) < 1e-9 * 200
+        _check(an, g, st)
+        assert st.best_total <= st.cur_total
+
+
+def test_profile_matches_bfs(gpu):
+    g = graphs.random_regular(300, 5, 2)
+    with gg.Annealer(g, candidates=16, proposals=64, compose=4, seed=5) as an:
+        assert np.array_equal(an.profile(), oracle.level_stats(g.adj))
+        an.run(20)
+        adj = graphs.create_adj(g.nodes, g.degree, an.edges())
+        assert np.array_equal(an.profile(), oracle.level_stats(adj))
+
+
+def test_target_stops_the_loop(gpu):
+    g = graphs.random_regular(512, 6, 12)
+    with gg.Annealer(g, candidates=16, compose=8, seed=2) as an:
+        st0 = an.run(0)
+        goal = st0.cur_total - 200
+        an.target(st0.cur_diam, goal)
+        st = st0
+        for _ in range(50):
+            st = an.run(8)
+            if st.done:
+                break
+        assert st.done and st.cur_total <= goal
+        again = an.run(8)
+        assert (again.step, again.cur_total) == (st.step, st.cur_total)
+        _check(an, g, again)
+
+
+def test_large_learned_step(gpu):
+    """The filter's full configuration: 4096 proposals, 64 evaluated."""
+    g = graphs.random_regular(2048, 12, 7)
+    with gg.Annealer(g, candidates=64, proposals=4096, compose=32, seed=4) as an:
+        st = an.run(6)
+        _check(an, g, st)
+        assert st.evals == 6 * (64 + 4 + 1)   # candidates, predicted composites, exact composite
+
+
+def test_bad_inputs(gpu):
+    g = graphs.random_regular(64, 4, 1)
+    bad = g.edges.copy()
+    bad[0, 1] = bad[0, 0]                        # self-loop
+    with pytest.raises(gg.EvaluationError):
+        gg.Annealer(graphs.Graph(g.nodes, g.degree, bad, g.adj))
+    with pytest.raises(gg.EvaluationError):
+        gg.Annealer(g, candidates=0)
+    with pytest.raises(gg.EvaluationError):
+        gg.Annealer(g, candidates=16, proposals=100)   # not a multiple of 16
+    with pytest.raises(gg.EvaluationError):
+        gg.Annealer(g, candidates=10, proposals=64)    # filtered candidates: multiple of 16
+    two = np.concatenate([g.edges, g.edges + 64])       # two components
+    gd = graphs.Graph(128, 4, two.astype(np.int32), graphs.create_adj(128, 4, two))
+    with pytest.raises(gg.EvaluationError):
+        gg.Annealer(gd)
+
+
+def test_filter_beats_random_selection(gpu):
+    """What the trained network gains: after online training, the swaps it
+    ranks highest improve the exact distance total far more often than the
+    swaps drawn at random in the same steps (the last quarter of every
+    step's evaluated candidates), and their exact changes are lower."""
+    g = graphs.random_regular(2048, 12, 2)
+    K = 64
+    nt = K - K // 4
+    with gg.Annealer(g, candidates=K, proposals=4096, compose=64, seed=1) as an:
+        an.run(150)                                  # online training
+        top, rnd = [], []
+        for _ in range(60):
+            an.run(1)
+            p, lab = an.last_step()
+            top.append(lab[:nt])
+            rnd.append(lab[nt:])
+        top, rnd = np.concatenate(top), np.concatenate(rnd)
+        assert np.mean(top < 0) > 1.5 * np.mean(rnd < 0)
+        assert top.mean() < rnd.mean()
+        _check(an, g, an.run(0))
