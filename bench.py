@@ -21,6 +21,13 @@ total, ASPL) of that graph.
 * ``cpu_baseline`` -- the reference's own OpenMP evaluator (compiled from its
   sources into oracle/_ref) on this host's cores, over a bounded sample.
 
+* ``batch`` -- the mixed batch (a 4096-vertex base graph and 256 single-swap
+  candidates of 512..16384-vertex graphs) in one autotuned launch: graphs/s,
+  e2e, roofline of the batch kernel.
+* ``sa`` -- the annealing race at N=16384, d=12: wall seconds of plain device
+  annealing (the reference's one-candidate step) for a fixed number of steps,
+  and of the batched+learned annealer to reach the same exact distance total.
+
 ``--impl reference`` times that reference CPU evaluator alone (all host
 threads) on the same workload and prints its own line.
 
@@ -234,6 +241,9 @@ def main() -> int:
     ap.add_argument("--workload", default="n65536d16", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ref-gpu", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="skip the mixed-batch measurement")
+    ap.add_argument("--no-sa", action="store_true", help="skip the annealing race")
+    ap.add_argument("--sa-plain-steps", type=int, default=30000, help="plain annealing steps that set the target")
     ap.add_argument("--flush-mib", type=int, default=512, help="L2 flush buffer written before every step")
     ap.add_argument("--window-bits", type=int, default=0, help="force the source-window width (0 = automatic)")
     ap.add_argument("--ball", type=int, default=-1, choices=[-1, 0, 1],
@@ -391,12 +401,109 @@ def main() -> int:
         line["cpu_baseline"] = cpu_baseline(host_adj)
     if rank == 0 and world == 1 and not args.no_ref_gpu and groups == 1:
         line["reference_cuda"] = reference_cuda(host_adj, first)
+    if rank == 0 and world == 1 and not args.no_batch:
+        line["batch"] = batch_bench(peak, lib)
+    if rank == 0 and world == 1 and not args.no_sa:
+        line["sa"] = sa_bench(args.sa_plain_steps)
     if rank == 0:
         print(json.dumps(line))
     if dist:
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def batch_bench(peak: float, lib) -> dict:
+    """The mixed batch: a 4096-vertex 12-regular base graph and 256 seeded
+    2-opt candidates of 12-regular graphs with 512..16384 vertices, all in one
+    cooperative launch replayed from a CUDA graph, plan autotuned.  value =
+    graphs per second with the adjacency resident (launch timed with CUDA
+    events by the library); e2e = host arrays in, results out."""
+    import graphgolf_b200 as gg
+    from graphgolf_b200 import graphs
+    w = graphs.batch_workload()
+    adjs = [x.adj for x in w]
+    b = gg.Batch([x.nodes for x in w], 12)
+    b.upload(adjs)
+    t0 = time.perf_counter()
+    bits, team, _ = b.autotune(2)
+    tune_s = time.perf_counter() - t0
+    b.launch()
+    res = b.collect()
+    for i in (0, 1, len(w) // 2, len(w) - 1):   # spot check against the single-graph evaluator
+        r = gg.evaluate(adjs[i])
+        assert (r.diameter, r.total) == (res[i].diameter, res[i].total)
+    ms = []
+    for _ in range(10):
+        b.launch()
+        b.collect()
+        ms.append(b.kernel_ms())
+    t0 = time.perf_counter()
+    for _ in range(5):
+        b.evaluate(adjs)
+    e2e_ms = (time.perf_counter() - t0) / 5 * 1e3
+    kms = statistics.median(ms)
+    alg = sum(sweep_bytes(x.nodes, 12, r.dense_levels, r.window_bits) for x, r in zip(w, res))
+    achieved = alg / (kms / 1e3) / 1e9
+    l2 = C.c_double(0)
+    l2_ok = lib.ggb_probe_l2_gather(16384, 12, bits, 10, C.byref(l2)) == 0
+    b.close()
+    return {"workload": "4096-vertex base + 256 single-swap candidates, d=12, N log-uniform 512..16384",
+            "graphs": len(w), "plan": {"window_bits": bits, "team_ctas": team, "autotune_s": tune_s},
+            "value": len(w) / (kms / 1e3), "unit": "graphs/s", "ms_per_batch": kms,
+            "e2e": {"value": len(w) / (e2e_ms / 1e3), "unit": "graphs/s", "ms_per_batch": e2e_ms,
+                    "h2d_bytes_per_step": int(sum(a.nbytes for a in adjs)), "d2h_bytes_per_step": 48 * len(w)},
+            "roofline": {"bound": "hbm", "kernel": f"apsp_batch_kernel<{bits // 128}>", "achieved": achieved,
+                         "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "algorithmic_bytes_per_launch": alg,
+                         "l2_gather_peak_gbs": l2.value if l2_ok else None,
+                         "frac_of_l2_gather_peak": achieved / l2.value if l2_ok and l2.value else None},
+            "checked": "4 graphs bit-identical to the single-graph evaluator"}
+
+
+def sa_bench(plain_steps: int) -> dict:
+    """Annealing race on a seeded random 12-regular graph, N=16384 (hill
+    climbing, the reference's -H rule).  Plain device annealing (one random
+    2-opt candidate per step, evaluated in full: the reference's step) runs
+    plain_steps steps; its final exact distance total is the target.  The
+    batched+learned annealer (4096 proposals per step ranked by the trained
+    network, the best 256 evaluated exactly against the base, the disjoint
+    exact improvers composed and evaluated in full) and the batched one
+    without the network then run until they reach the same exact total.
+    Wall seconds on the host clock around the runs (each run synchronises)."""
+    import graphgolf_b200 as gg
+    from graphgolf_b200 import graphs
+    g = graphs.random_regular(16384, 12, 2)
+    out = {"workload": "random 12-regular, N=16384, hill climbing, seed 2", "plain_steps": plain_steps}
+    an = gg.Annealer(g, 1, 1, 0, seed=1)
+    st0 = an.run(0)
+    t0 = time.perf_counter()
+    st = an.run(plain_steps)
+    t_plain = time.perf_counter() - t0
+    an.close()
+    out["start_aspl"] = st0.cur_aspl
+    out["target_aspl"] = st.cur_aspl
+    out["target_total"] = st.cur_total
+    out["plain"] = {"wall_s": t_plain, "steps": st.step, "accepts": st.accepts, "evals": st.evals}
+    for name, K, G in (("learned", 256, 4096), ("batched", 256, 256)):
+        a = gg.Annealer(g, K, G, K, seed=1)
+        if G > K:
+            a.predicted(0, 1)
+        a.target(st.cur_diam, st.cur_total)
+        s = a.run(0)
+        t0 = time.perf_counter()
+        while not s.done and time.perf_counter() - t0 < 90:
+            s = a.run(10)
+        el = time.perf_counter() - t0
+        edges = a.edges()
+        a.close()
+        adj = graphs.create_adj(g.nodes, g.degree, edges)
+        r = gg.evaluate(adj)
+        out[name] = {"wall_s": el, "reached": bool(s.done), "steps": s.step, "accepts": s.accepts,
+                     "moved_swaps": s.moved_swaps, "evals": s.evals, "final_aspl": s.cur_aspl,
+                     "final_checked": (r.diameter, r.total) == (s.cur_diam, s.cur_total),
+                     "candidates": K, "proposals": G, "speedup_vs_plain": t_plain / el if s.done else None}
+    return out
 
 
 def reference_cuda(adj, want):

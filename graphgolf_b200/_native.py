@@ -58,6 +58,7 @@ class ggb_sa_stats(C.Structure):
         ("moved_swaps", C.c_longlong),
         ("evals", C.c_longlong),
         ("pred_accepts", C.c_longlong),
+        ("unevaluated", C.c_longlong),
         ("cur_diam", C.c_int),
         ("best_diam", C.c_int),
         ("cur_total", C.c_longlong),
@@ -126,11 +127,13 @@ CORE_SIGNATURES = {
     "ggb_sa_destroy": (None, [_P]),
     "ggb_sa_set_schedule": (_I, [_P, C.c_double, C.c_double, _I]),
     "ggb_sa_set_target": (_I, [_P, _I, _LL]),
+    "ggb_sa_set_predicted": (_I, [_P, _I, _I]),
     "ggb_sa_autotune": (_I, [_P, _I, _IP, _IP, C.POINTER(C.c_double)]),
     "ggb_sa_run": (_I, [_P, _LL, C.POINTER(ggb_sa_stats)]),
     "ggb_sa_edges": (_I, [_P, _I, _P]),
     "ggb_sa_profile": (_I, [_P, _P]),
     "ggb_sa_last_step": (_I, [_P, _P, _P]),
+    "ggb_sa_check_delta": (_I, [_P, _IP, _IP, _IP]),
 }
 
 HOST_SIGNATURES = {

@@ -29,6 +29,7 @@ class Stats:
     moved_swaps: int
     evals: int
     pred_accepts: int
+    unevaluated: int
     cur_diam: int
     best_diam: int
     cur_total: int
@@ -73,6 +74,10 @@ class Annealer:
     def schedule(self, temp: float = 0.0, cooling: float = 1.0, hill_climbing: bool = True) -> None:
         _raise(self._lib.ggb_sa_set_schedule(self._h, temp, cooling, 1 if hill_climbing else 0))
 
+    def predicted(self, composites: int = 4, max_swaps: int = 64) -> None:
+        """Predicted composites per step (filter only) and the largest's size."""
+        _raise(self._lib.ggb_sa_set_predicted(self._h, composites, max_swaps))
+
     def target(self, diameter: int, total: int) -> None:
         _raise(self._lib.ggb_sa_set_target(self._h, diameter, total))
 
@@ -84,8 +89,8 @@ class Annealer:
     def run(self, steps: int) -> Stats:
         st = ggb_sa_stats()
         _raise(self._lib.ggb_sa_run(self._h, steps, C.byref(st)))
-        return Stats(st.step, st.accepts, st.multi_accepts, st.moved_swaps, st.evals, st.pred_accepts, st.cur_diam,
-                     st.best_diam,
+        return Stats(st.step, st.accepts, st.multi_accepts, st.moved_swaps, st.evals, st.pred_accepts,
+                     st.unevaluated, st.cur_diam, st.best_diam,
                      st.cur_total, st.best_total, st.cur_aspl, st.best_aspl, st.temp, bool(st.done))
 
     def edges(self, best: bool = False) -> np.ndarray:
@@ -100,6 +105,13 @@ class Annealer:
         lb = np.empty(k, dtype=np.float32)
         _raise(self._lib.ggb_sa_last_step(self._h, pr.ctypes.data, lb.ctypes.data))
         return pr, lb
+
+    def check_delta(self) -> tuple[int, int, int]:
+        """(compared, mismatches, unevaluated): fresh candidates evaluated
+        against the base and in full."""
+        c, m, u = C.c_int(), C.c_int(), C.c_int()
+        _raise(self._lib.ggb_sa_check_delta(self._h, C.byref(c), C.byref(m), C.byref(u)))
+        return c.value, m.value, u.value
 
     def profile(self) -> np.ndarray:
         """[nodes][32]: entry [v][k] = vertices farther than k from v."""

@@ -344,6 +344,10 @@ int launch_apsp(const int* d_adj, int N, int d, int n_src1, int split, int ac, i
   a.win_stride = procs;
   a.phantom = g.phantom;
   a.stats = nullptr;
+  a.levels = nullptr;
+  a.level_counts = nullptr;
+  a.win_levels = nullptr;
+  a.level_cap = 0;
   a.trace = g.d_trace;
   a.trace_cap = g.trace_cap;
   a.vec4 = vec4 ? 1 : 0;

@@ -1,0 +1,379 @@
+// apsp_delta.cuh -- exact evaluation of 2-opt candidates relative to a base.
+//
+// A 2-opt swap changes four adjacency entries, and only a few thousand of
+// the N^2 distances.  The base build (apsp_base_kernel) evaluates the
+// current graph once with windows of 128 sources and keeps every level's
+// bitset rows S_k, each level's popcount and each window's completion level.
+// A candidate is then evaluated window by window from the base alone:
+//
+//   S'_0 = S_0 (the identity), and for k >= 0
+//   S'_{k+1}[v] = S'_k[v] | OR_{u in N'(v)} S'_k[u]          (the recurrence of
+//                                                             apsp_kernel.cuh)
+//
+// S'_{k+1}[v] can differ from S_{k+1}[v] only if v's neighbour list changed
+// (the four endpoints P) or v or one of its neighbours differed at level k.
+// So level k+1 is re-derived only on P, the dirty set D_k = {v : S'_k[v] !=
+// S_k[v]} and the neighbours of D_k; rows that come out equal to the base are
+// dropped, the others form D_{k+1}, and the level's popcount changes by
+// delta_{k+1} = sum over D_{k+1} of popc(S'_{k+1}[v]) - popc(S_{k+1}[v]).
+// With C_k the base counts (N*l from the base's completion level on), the
+// candidate's window is complete at the first k with C_k + delta_k == N*l,
+// and its distance sum is the base's minus sum_k delta_k -- the same
+// integers the full evaluation produces (general/evaluation.c:183-200 per
+// level).  A stall (a level that adds nothing before completion) is a
+// disconnected candidate.  A window whose dirty set outgrows the task's
+// shared memory (typically one holding a swap endpoint, whose own distances
+// change for many vertices) continues as a dense sweep of that window alone,
+// in a slot of a scratch pool; only when the pool is exhausted does it
+// report "not evaluated" instead of guessing.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "apsp_kernel.cuh"
+
+namespace ggb {
+
+// One 2-opt swap in canonical form: lines line[0] = {x0,x1} and
+// line[1] = {x2,x3} become {x0,x2} and {x1,x3}.  pos[k] is the slot of row
+// x_k whose entry changes: row x0: x1 -> x2, row x1: x0 -> x3,
+// row x2: x3 -> x0, row x3: x2 -> x1.  A valid swap has 4 distinct endpoints.
+struct Swap {
+  int line[2];
+  int x[4];
+  int pos[4];
+  int valid;
+  int pad_;
+};
+
+// ---- the base build: one graph, windows split over CTA teams, levels kept ------
+struct BaseResult {
+  long long sum;          // the graph's distance sum before + N(N-1)
+  int diam;
+  int disconnected;
+  int bad;                // windows whose levels did not fit (or that stalled)
+  int pad_;
+};
+
+struct BaseArgs {
+  ApspCtrl* grid_ctrl;    // one barrier over the whole launch, zeroed before it
+  ApspCtrl* team_ctrl;    // [n_teams], zeroed before the launch
+  uint4* scratch;         // team t: 2*N*R cells at scratch + t*2*N*R
+  BaseResult* result;     // written by the launch
+  const int* gate;        // the launch does nothing while *gate == 0 (null: always runs)
+  int* sticky;            // first error code (never cleared here)
+  int n_teams, team_ctas;
+};
+
+// Team t evaluates windows t, t + n_teams, ... of the graph in `a` (phase 1
+// only), writing their levels, counts and completion levels into a's level
+// arrays and, when a.stats is set, the per-vertex statistics.
+template <int R>
+__global__ void __launch_bounds__(kThreads, 1) apsp_base_kernel(ApspArgs a, const BaseArgs b) {
+  __shared__ ApspSmem sm;
+  extern __shared__ unsigned s_dyn[];
+  if (b.gate && ld_volatile_i32(b.gate) == 0) return;   // written before the launch: the same in every CTA
+  const long long n_tid = (long long)gridDim.x * blockDim.x;
+  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (a.stats)
+    for (long long i = tid; i < (long long)a.N * kStatLevels; i += n_tid) a.stats[i] = 0u;
+  if (tid == 0) {
+    b.result->sum = 0;
+    b.result->diam = 1;
+    b.result->disconnected = 0;
+    b.result->bad = 0;
+  }
+  if (threadIdx.x < 8) sm.seen[threadIdx.x >> 1][threadIdx.x & 1] = 0ULL;
+  unsigned long long gt = gridDim.x;
+  if (!grid_barrier(b.grid_ctrl, gt, a.timeout_ns, &sm.flag)) {
+    if (b.sticky && threadIdx.x == 0) atomicCAS(b.sticky, 0, kErrTimeout);
+    return;
+  }
+  const int team = (int)blockIdx.x / b.team_ctas, cta = (int)blockIdx.x % b.team_ctas;
+  if (team >= b.n_teams) return;
+  a.ctrl = b.team_ctrl + team;
+  a.win_first = team;
+  a.win_stride = b.n_teams;
+  a.buf0 = b.scratch + (size_t)team * 2 * a.N * R;
+  a.buf1 = a.buf0 + (size_t)a.N * R;
+  unsigned long long bar_target = 0;
+  unsigned gl = 0;
+  int ntrace = 0;
+  EvalOut o;
+  const bool ok = a.stats ? eval_windows<R, true>(a, cta, b.team_ctas, sm, s_dyn, bar_target, gl, ntrace, o)
+                          : eval_windows<R, false>(a, cta, b.team_ctas, sm, s_dyn, bar_target, gl, ntrace, o);
+  if (!ok) {
+    if (b.sticky && threadIdx.x == 0) atomicCAS(b.sticky, 0, max(1, ld_volatile_i32(&a.ctrl->error)));
+    return;
+  }
+  if (cta == 0 && threadIdx.x == 0 && o.windows > 0) {
+    atomicAdd(reinterpret_cast<unsigned long long*>(&b.result->sum), (unsigned long long)o.sum);
+    atomicMax(&b.result->diam, o.diam);
+    atomicOr(&b.result->disconnected, o.disconnected);
+  }
+}
+
+// ---- the delta evaluation: one CTA per (candidate, window) -----------------------
+constexpr int kDeltaThreads = 256;
+constexpr int kDeltaRows = 512;        // dirty rows a task can hold per level
+constexpr int kDeltaHash = 1024;       // hash slots for the dirty rows (power of two)
+constexpr int kDeltaLevels = 48;       // levels a task may run past level 0
+
+struct DeltaArgs {
+  const uint4* levels;                 // base rows, R = 1: [nwin][level_cap + 1][N]
+  const long long* level_counts;       // [nwin][level_cap + 1]
+  const int* win_levels;               // [nwin]
+  const int* adj;                      // base adjacency [N][d]
+  const Swap* sw;
+  const int* sel;                      // candidate c is sw[sel[c]] (sw[c] when null)
+  const int* stop;                     // nothing runs while *stop != 0 (may be null)
+  long long* dsum;                     // [K][nwin] sum_k delta_k
+  int* dlev;                           // [K][nwin] completion level; -1 stalled; -2 not evaluated
+  uint4* dense_pool;                   // dense_slots slots of 2*N rows for tasks whose dirty set overflows
+  int* dense_used;                     // slots taken (zeroed before the launch)
+  int dense_slots;
+  int N, d, nwin, n_src, level_cap, K;
+};
+
+__device__ __forceinline__ uint4 identity_row(int v, int base, int l) {
+  const unsigned b = (unsigned)(v - base);
+  uint4 r = make_uint4(0u, 0u, 0u, 0u);
+  if (b < (unsigned)l) {
+    const unsigned m = 1u << (b & 31);
+    const int wd = (int)(b >> 5);
+    r.x = wd == 0 ? m : 0u;
+    r.y = wd == 1 ? m : 0u;
+    r.z = wd == 2 ? m : 0u;
+    r.w = wd == 3 ? m : 0u;
+  }
+  return r;
+}
+
+__global__ void __launch_bounds__(kDeltaThreads) delta_kernel(const DeltaArgs a) {
+  extern __shared__ unsigned s_claim[];                 // [ceil(N/32)]: rows claimed this level
+  __shared__ int s_ids[2][kDeltaRows];
+  __shared__ uint4 s_val[2][kDeltaRows];
+  __shared__ int s_key[kDeltaHash];
+  __shared__ int s_slot[kDeltaHash];
+  __shared__ int s_n[2];
+  __shared__ int s_over;
+  __shared__ unsigned long long s_red[kDeltaThreads / 32];
+  if (a.stop && ld_volatile_i32(a.stop) != 0) return;
+  const int c = blockIdx.x / a.nwin, w = blockIdx.x % a.nwin;
+  const Swap sw = a.sw[a.sel ? a.sel[c] : c];
+  const int N = a.N, d = a.d;
+  const int base = w * 128;
+  const int l = min(128, a.n_src - base);
+  const long long full_count = (long long)N * l;
+  const int L = a.win_levels[w];
+  long long* const out_sum = a.dsum + (size_t)c * a.nwin + w;
+  int* const out_lev = a.dlev + (size_t)c * a.nwin + w;
+  if (!sw.valid || L < 0) {            // no change, or a base window that cannot serve
+    if (threadIdx.x == 0) {
+      *out_sum = 0;
+      *out_lev = sw.valid ? -2 : L;
+    }
+    return;
+  }
+  const uint4 fullm = chunk_full_mask(0, l);
+  const int cap = a.level_cap;
+  const uint4* const lev = a.levels + (size_t)w * (cap + 1) * N;
+  const long long* const lc = a.level_counts + (size_t)w * (cap + 1);
+  const int nclaim = (N + 31) / 32;
+  for (int i = threadIdx.x; i < nclaim; i += blockDim.x) s_claim[i] = 0u;
+  for (int i = threadIdx.x; i < kDeltaHash; i += blockDim.x) s_key[i] = -1;
+  if (threadIdx.x == 0) {
+    s_n[0] = 0;
+    s_n[1] = 0;
+    s_over = 0;
+  }
+  __syncthreads();
+  const int X0 = sw.x[0], X1 = sw.x[1], X2 = sw.x[2], X3 = sw.x[3];
+  const int NV[4] = {X2, X3, X0, X1};
+  // candidate neighbour j of row x
+  auto nb = [&](int x, int j) -> int {
+    const int q = x == X0 ? 0 : x == X1 ? 1 : x == X2 ? 2 : x == X3 ? 3 : -1;
+    if (q >= 0 && j == sw.pos[q]) return NV[q];
+    return __ldg(a.adj + (long long)x * d + j);
+  };
+  auto base_row = [&](int k, int v) -> uint4 {
+    if (k == 0) return identity_row(v, base, l);
+    if (k > L) return fullm;
+    return __ldg(lev + (size_t)k * N + v);
+  };
+  // S'_k of row y: its dirty value when y is in D_k (table s_key), else the base
+  auto row_k = [&](int k, int nd, int cur, int y) -> uint4 {
+    if (nd > 0) {
+      unsigned h = ((unsigned)y * 2654435761u) & (kDeltaHash - 1);
+      for (int p = 0; p < kDeltaHash; ++p) {
+        const int key = s_key[h];
+        if (key == y) return s_val[cur][s_slot[h]];
+        if (key < 0) break;
+        h = (h + 1) & (kDeltaHash - 1);
+      }
+    }
+    return base_row(k, y);
+  };
+  int cur = 0;
+  long long total_delta = 0, prev_count = l;
+  int Lc = -1;
+  int status = -2;   // becomes the completion level, or -1 when the candidate stalls
+  int k = 0;
+  bool dense = false;
+  for (; k < kDeltaLevels; ++k) {
+    const int nd = s_n[cur];
+    const int nxt = cur ^ 1;
+    const int items = 4 + nd * (d + 1);
+    unsigned long long pos_cnt = 0, neg_cnt = 0;
+    for (int it = threadIdx.x; it < items; it += blockDim.x) {
+      int x;
+      if (it < 4) {
+        x = sw.x[it];
+      } else {
+        const int q = (it - 4) / (d + 1), j = (it - 4) % (d + 1);
+        const int v = s_ids[cur][q];
+        x = j == d ? v : nb(v, j);
+      }
+      const unsigned bit = 1u << (x & 31);
+      if (atomicOr(&s_claim[x >> 5], bit) & bit) continue;
+      uint4 acc = row_k(k, nd, cur, x);
+      for (int j = 0; j < d; ++j) or_into(acc, row_k(k, nd, cur, nb(x, j)));
+      const uint4 bn = base_row(k + 1, x);
+      if (!equal4(acc, bn)) {
+        const int idx = atomicAdd(&s_n[nxt], 1);
+        if (idx < kDeltaRows) {
+          s_ids[nxt][idx] = x;
+          s_val[nxt][idx] = acc;
+        } else {
+          s_over = 1;
+        }
+        const unsigned pa = popc4(acc), pb = popc4(bn);
+        if (pa > pb) pos_cnt += pa - pb; else neg_cnt += pb - pa;
+      }
+    }
+    __syncthreads();
+    // clear the claims (every claimed row lies in a word some item touched)
+    for (int it = threadIdx.x; it < items; it += blockDim.x) {
+      int x;
+      if (it < 4) {
+        x = sw.x[it];
+      } else {
+        const int q = (it - 4) / (d + 1), j = (it - 4) % (d + 1);
+        const int v = s_ids[cur][q];
+        x = j == d ? v : nb(v, j);
+      }
+      s_claim[x >> 5] = 0u;
+    }
+    // delta_{k+1} = pos - neg, reduced over the block
+    long long dl = (long long)pos_cnt - (long long)neg_cnt;
+    for (int o = 16; o > 0; o >>= 1) dl += __shfl_xor_sync(0xffffffffu, dl, o);
+    if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = (unsigned long long)dl;
+    __syncthreads();
+    if (s_over) { dense = true; break; }   // D_k and its table are still intact
+    long long delta = 0;
+    for (int i = 0; i < kDeltaThreads / 32; ++i) delta += (long long)s_red[i];
+    // the next level's lookup table
+    for (int i = threadIdx.x; i < kDeltaHash; i += blockDim.x) s_key[i] = -1;
+    __syncthreads();
+    const int nn = s_n[nxt];
+    for (int i = threadIdx.x; i < nn; i += blockDim.x) {
+      const int y = s_ids[nxt][i];
+      unsigned h = ((unsigned)y * 2654435761u) & (kDeltaHash - 1);
+      while (atomicCAS(&s_key[h], -1, y) != -1) h = (h + 1) & (kDeltaHash - 1);
+      s_slot[h] = i;
+    }
+    total_delta += delta;
+    const long long ck = (k + 1 <= L) ? lc[k + 1] : full_count;
+    const long long count = ck + delta;
+    if (Lc < 0 && count == full_count) Lc = k + 1;
+    __syncthreads();
+    if (threadIdx.x == 0) s_n[cur] = 0;
+    if (Lc >= 0 && k + 1 >= L) { status = Lc; break; }
+    if (Lc < 0 && count == prev_count) { status = -1; break; }
+    prev_count = count;
+    cur = nxt;
+    __syncthreads();
+  }
+  if (dense) {
+    // The dirty set outgrew shared memory while deriving level k+1: from
+    // S'_k (the base with D_k's rows) the window is swept in full, level by
+    // level, in a slot of the pool; counts are exact popcounts.
+    __shared__ int s_pool;
+    if (threadIdx.x == 0) s_pool = atomicAdd(a.dense_used, 1);
+    __syncthreads();
+    const int slot = s_pool;
+    if (slot < a.dense_slots) {
+      uint4* A = a.dense_pool + (size_t)slot * 2 * N;
+      uint4* B = A + N;
+      const int nd = s_n[cur];
+      for (int v = threadIdx.x; v < N; v += blockDim.x) __stcg(A + v, row_k(k, nd, cur, v));
+      __syncthreads();
+      for (; k < kDeltaLevels; ++k) {
+        unsigned long long cnt = 0;
+        for (int v = threadIdx.x; v < N; v += blockDim.x) {
+          uint4 acc = __ldcg(A + v);
+          for (int j = 0; j < d; ++j) or_into(acc, __ldcg(A + nb(v, j)));
+          __stcg(B + v, acc);
+          cnt += popc4(acc);
+        }
+        for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+        __syncthreads();
+        if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = cnt;
+        __syncthreads();
+        long long count = 0;
+        for (int i = 0; i < kDeltaThreads / 32; ++i) count += (long long)s_red[i];
+        const long long ck = (k + 1 <= L) ? lc[k + 1] : full_count;
+        total_delta += count - ck;
+        if (Lc < 0 && count == full_count) Lc = k + 1;
+        if (Lc >= 0 && k + 1 >= L) { status = Lc; break; }
+        if (Lc < 0 && count == prev_count) { status = -1; break; }
+        prev_count = count;
+        uint4* t = A;
+        A = B;
+        B = t;
+        __syncthreads();
+      }
+    }
+  }
+  if (threadIdx.x == 0) {
+    *out_sum = total_delta;
+    *out_lev = status;
+  }
+}
+
+// Per candidate: the base's result changed by its windows' deltas, as the
+// record a batch evaluation writes (done = 0 when a window was not
+// evaluated).  One warp per candidate.
+__global__ void delta_reduce_kernel(const DeltaArgs a, const BaseResult* __restrict__ base, BatchOut* __restrict__ out) {
+  const int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (c >= a.K) return;
+  if (a.stop && ld_volatile_i32(a.stop) != 0) return;
+  long long s = 0;
+  int mx = 0, stalled = 0, missing = 0;
+  for (int w = lane; w < a.nwin; w += 32) {
+    s += a.dsum[(size_t)c * a.nwin + w];
+    const int lv = a.dlev[(size_t)c * a.nwin + w];
+    if (lv == -1) stalled = 1;
+    else if (lv < 0) missing = 1;
+    else mx = max(mx, lv);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    s += __shfl_xor_sync(0xffffffffu, s, o);
+    mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    stalled |= __shfl_xor_sync(0xffffffffu, stalled, o);
+    missing |= __shfl_xor_sync(0xffffffffu, missing, o);
+  }
+  if (lane == 0) {
+    BatchOut r;
+    r.sum = base->sum - s;
+    r.levels = 0;
+    r.dense_levels = 0;
+    r.diam = stalled ? a.N + 1 : mx;
+    r.disconnected = stalled;
+    r.windows = a.nwin;
+    r.done = (missing || base->disconnected) ? 0 : 1;
+    out[c] = r;
+  }
+}
+
+}  // namespace ggb

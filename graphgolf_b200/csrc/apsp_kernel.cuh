@@ -91,6 +91,15 @@ struct ApspArgs {
   int phantom;           // extra arrivals every barrier waits for: 0 in normal use; the
                          // fault-path test sets 1 so that every bounded wait runs out
   unsigned* stats;       // profile kernel only: [N][kStatLevels] unreached sources per level
+  // base builds only (null otherwise): every level's rows of window t at
+  // levels + (t * (level_cap + 1) + k) * N * R for k <= level_cap, the
+  // level's popcount at level_counts[t * (level_cap + 1) + k], and the
+  // window's completion level (first k with S_k full; -1 if it stalls) at
+  // win_levels[t]
+  uint4* levels;
+  long long* level_counts;
+  int* win_levels;
+  int level_cap;
 };
 
 __device__ __forceinline__ unsigned long long globaltimer_ns() {
@@ -391,7 +400,7 @@ template <int R, int VEC, bool STATS = false>
 __device__ __forceinline__ void seed_window(const ApspArgs& a, const int* __restrict__ adj, int base, int l,
                                             uint4* s2_out, int* s_nb,
                                             unsigned* s_rw, unsigned (&c)[4], bool& adj_ok, long long warp_id,
-                                            long long n_warps) {
+                                            long long n_warps, uint4* s1_out = nullptr) {
   constexpr int SROW = 4 * R;
   const int N = a.N, d = a.d;
   const int lane = threadIdx.x & 31, g = lane / kSeedGroup, r = lane % kSeedGroup;
@@ -430,6 +439,7 @@ __device__ __forceinline__ void seed_window(const ApspArgs& a, const int* __rest
         uint4 x2 = rows4[(2 * i + 1) * R + col];
         or_into(x2, x1);   // S_2 includes S_1
         st_cg(s2_out + vi * R + col, x2);
+        if (s1_out) st_cg(s1_out + vi * R + col, x1);
         c1 += popc4(x1);
         c2 += popc4(x2);
       }
@@ -438,9 +448,9 @@ __device__ __forceinline__ void seed_window(const ApspArgs& a, const int* __rest
         const unsigned t1 = __reduce_add_sync(0xffffffffu, c1), t2 = __reduce_add_sync(0xffffffffu, c2);
         if (lane == 0) {
           unsigned* st = a.stats + vi * kStatLevels;
-          st[0] += (unsigned)l - ((unsigned)(vi - base) < (unsigned)l ? 1u : 0u);
-          st[1] += (unsigned)l - t1;
-          st[2] += (unsigned)l - t2;
+          atomicAdd(st + 0, (unsigned)l - ((unsigned)(vi - base) < (unsigned)l ? 1u : 0u));
+          atomicAdd(st + 1, (unsigned)l - t1);
+          atomicAdd(st + 2, (unsigned)l - t2);
         }
       }
     }
@@ -640,7 +650,7 @@ __device__ __forceinline__ void sweep_wide(const uint4* __restrict__ src, uint4*
     if (v < split) cl[0] += cc; else cl[1] += cc;
     if constexpr (STATS) {
       const unsigned tot = __reduce_add_sync(0xffffffffu, cc);
-      if (lane == 0 && lvl < kStatLevels) stats[v * kStatLevels + lvl] += (unsigned)l - tot;
+      if (lane == 0 && lvl < kStatLevels) atomicAdd(stats + v * kStatLevels + lvl, (unsigned)l - tot);
     }
   }
 }
@@ -726,6 +736,11 @@ __device__ __forceinline__ bool eval_windows(const ApspArgs& a, int cta, int nct
       const uint4* cur;           // S_kk rows the next sweep gathers from
       uint4* nxt;                 // rows it writes
       bool own_count = false;     // the first sweep of a ball window also reports S_3
+      // base builds: this window's level rows and counts (never with the ball pre-pass)
+      uint4* const lev0 = a.levels ? a.levels + (size_t)t * (a.level_cap + 1) * N * R : nullptr;
+      long long* const lcnt = a.levels ? a.level_counts + (size_t)t * (a.level_cap + 1) : nullptr;
+      const bool rec = lev0 && cta == 0 && threadIdx.x == 0;
+      bool lev_over = false;
       if (use_ball) {
         // ---- levels 0 and 1 from the ball pre-pass; S_3 rows are in HBM --------
         const unsigned long long* bc = a.ball_cnt + (size_t)local * 6;
@@ -742,10 +757,12 @@ __device__ __forceinline__ bool eval_windows(const ApspArgs& a, int cta, int nct
       } else {
         // ---- levels 0 and 1 by two-hop seeding into buf0 -----------------------
         unsigned c[4] = {0u, 0u, 0u, 0u};  // S_1 lo, S_1 hi, S_2 lo, S_2 hi
+        uint4* const s2_out = lev0 ? lev0 + (size_t)2 * N * R : a.buf0;
+        uint4* const s1_out = lev0 ? lev0 + (size_t)N * R : nullptr;
         if (a.vec4)
-          seed_window<R, 4, STATS>(a, adjp, base, l, a.buf0, my_nb, my_rows, c, adj_ok, warp_id, n_warps);
+          seed_window<R, 4, STATS>(a, adjp, base, l, s2_out, my_nb, my_rows, c, adj_ok, warp_id, n_warps, s1_out);
         else
-          seed_window<R, 1, STATS>(a, adjp, base, l, a.buf0, my_nb, my_rows, c, adj_ok, warp_id, n_warps);
+          seed_window<R, 1, STATS>(a, adjp, base, l, s2_out, my_nb, my_rows, c, adj_ok, warp_id, n_warps, s1_out);
         if (!adj_ok) set_error(a.ctrl, kErrAdj, (int)blockIdx.x);
         cta_add_counts<4>(c, a.ctrl, gl, s_red);
         bar_target += grid;
@@ -765,14 +782,21 @@ __device__ __forceinline__ bool eval_windows(const ApspArgs& a, int cta, int nct
                                sum);
         }
         if (!act) kk = 2;
-        cur = a.buf0;
-        nxt = a.buf1;
+        if (rec) {
+          lcnt[0] = l;
+          lcnt[1] = seed_lvl[0] + seed_lvl[1];
+          lcnt[2] = seed_lvl[2] + seed_lvl[3];
+        }
+        cur = s2_out;
+        nxt = lev0 ? a.buf0 : a.buf1;
       }
       if (!act) {
         // ---- dense OR-gather sweeps ------------------------------------------------
         for (; kk < N; ++kk) {
           const uint4* __restrict__ src = cur;
-          uint4* __restrict__ dst = nxt;
+          const bool to_level = lev0 && kk + 1 <= a.level_cap;
+          if (lev0 && !to_level) lev_over = true;
+          uint4* __restrict__ dst = to_level ? lev0 + (size_t)(kk + 1) * N * R : nxt;
           unsigned cl[4] = {0u, 0u, 0u, 0u};   // new rows lo/hi, then (own_count) own rows lo/hi
           // The skipping sweep pays once the gathered level is nearly full
           // (its count, prev_total, is known); on denser-to-come levels the
@@ -834,7 +858,7 @@ __device__ __forceinline__ bool eval_windows(const ApspArgs& a, int cta, int nct
               unsigned tot = cc;
 #pragma unroll
               for (int o = LPR / 2; o > 0; o >>= 1) tot += __shfl_xor_sync(gmask, tot, o);
-              if (li == 0 && kk + 1 < kStatLevels) a.stats[v * kStatLevels + kk + 1] += (unsigned)l - tot;
+              if (li == 0 && kk + 1 < kStatLevels) atomicAdd(a.stats + v * kStatLevels + kk + 1, (unsigned)l - tot);
             }
           }
           if (!adj_ok) set_error(a.ctrl, kErrAdj, (int)blockIdx.x);
@@ -866,6 +890,7 @@ __device__ __forceinline__ bool eval_windows(const ApspArgs& a, int cta, int nct
             ++gl;
             ++levels;
             act = level_decision(phase, l0, l1, l, N, lo_rows, hi_rows, a.groups, prev_total, sum);
+            if (rec && kk + 1 <= a.level_cap) lcnt[kk + 1] = l0 + l1;
           }
           if (act) break;
           cur = dst;
@@ -874,6 +899,7 @@ __device__ __forceinline__ bool eval_windows(const ApspArgs& a, int cta, int nct
       }
       if (act == 2) { disconnected = 1; diam = N + 1; }
       else if (kk + 1 > diam) diam = (int)(kk + 1);
+      if (rec) a.win_levels[t] = act == 2 ? -1 : (lev_over ? -2 : (int)(kk + 1));
     }
   }
 
@@ -975,6 +1001,10 @@ __global__ void __launch_bounds__(kThreads, 1) apsp_batch_kernel(const BatchArgs
   a.trace_cap = 0;
   a.phantom = 0;
   a.stats = nullptr;
+  a.levels = nullptr;
+  a.level_counts = nullptr;
+  a.win_levels = nullptr;
+  a.level_cap = 0;
   unsigned long long bar_target = 0;
   unsigned gl = 0;
   int ntrace = 0;

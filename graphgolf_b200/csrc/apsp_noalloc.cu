@@ -174,6 +174,10 @@ extern "C" int ggb_eval_general_noalloc(int nodes, int based_nodes, int groups, 
   a.trace_cap = 0;
   a.phantom = 0;
   a.stats = nullptr;
+  a.levels = nullptr;
+  a.level_counts = nullptr;
+  a.win_levels = nullptr;
+  a.level_cap = 0;
 
   const int lpr = R >= 32 ? 32 : R;
   const int vpw = 32 / lpr;

@@ -38,6 +38,7 @@
 #include <vector>
 
 #include "../../include/graphgolf_b200.h"
+#include "apsp_delta.cuh"
 #include "batch_internal.h"
 #include "core_internal.h"
 #include "mlp_internal.h"
@@ -57,17 +58,7 @@ namespace sa {
 
 using bf16 = __nv_bfloat16;
 
-// One 2-opt swap in canonical form: lines line[0] = {x0,x1} and
-// line[1] = {x2,x3} become {x0,x2} and {x1,x3}.  pos[k] is the slot of row
-// x_k whose entry changes: row x0: x1 -> x2, row x1: x0 -> x3,
-// row x2: x3 -> x0, row x3: x2 -> x1.  A valid swap has 4 distinct endpoints.
-struct Swap {
-  int line[2];
-  int x[4];
-  int pos[4];
-  int valid;
-  int pad_;
-};
+using ggb::Swap;
 
 struct State {
   int N, d, lines, K;
@@ -83,7 +74,7 @@ struct State {
   int n_comp;            // swaps in this step's composite
   int best_k;            // rank-0 candidate of this step
   int pad_;
-  long long step, accepts, multi_accepts, moved_swaps, evals, best_step, pred_accepts;
+  long long step, accepts, multi_accepts, moved_swaps, evals, best_step, pred_accepts, unevaluated;
   int n_pred;            // swaps in this step's predicted list (learned mode)
   int pad2_;
   long long target_total;
@@ -249,14 +240,6 @@ __global__ void __launch_bounds__(kComposeThreads) compose_kernel(State* __restr
   s->n_comp = m;
 }
 
-// The composite graph: the current adjacency (copy), then its swaps.
-__global__ void copy_current_kernel(const State* __restrict__ s, int* __restrict__ dst) {
-  if (s->done) return;
-  const long long n = (long long)s->N * s->d;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-    dst[i] = s->adj[i];
-}
-
 // Size of predicted composite c: the first n_pred >> c swaps of the list.
 __device__ __forceinline__ int pred_size(int n_pred, int c) { return n_pred >> c; }
 
@@ -267,16 +250,13 @@ __device__ __forceinline__ void apply_swap(int* adj, int d, const Swap& w) {
   adj[(long long)w.x[3] * d + w.pos[3]] = w.x[1];
 }
 
-__global__ void patch_composite_kernel(const State* __restrict__ s, const Swap* __restrict__ comp,
-                                       int* __restrict__ dst) {
-  if (s->done) return;
-  for (int i = threadIdx.x; i < s->n_comp; i += blockDim.x) apply_swap(dst, s->d, comp[i]);
-}
 
 // ---- decide ---------------------------------------------------------------------------
 // general/sa.c:371-411 on exact totals: with groups = 1 the reference's
 // diff = (current_ASPL - new_ASPL) * N(N-1) is the change of the distance
 // total.  Threads k < K also write the training labels of this step.
+// comp_out (when there is a composite batch): [0] the exact composite,
+// [1 + c] predicted composite c.
 __global__ void decide_kernel(State* __restrict__ s, const Swap* __restrict__ sw, const int* __restrict__ sel,
                               const BatchOut* __restrict__ out, int K, const Swap* __restrict__ comp,
                               const BatchOut* __restrict__ comp_out, float* __restrict__ labels,
@@ -284,9 +264,10 @@ __global__ void decide_kernel(State* __restrict__ s, const Swap* __restrict__ sw
   if (s->done) return;
   const int N = s->N;
   const int k = threadIdx.x;
+  if (k < K && !out[k].done) atomicAdd(reinterpret_cast<unsigned long long*>(&s->unevaluated), 1ULL);
   if (labels && k < K) {
     const Key kk = key_of(out[k], N);
-    float lab = s->label_clip;
+    float lab = out[k].done ? s->label_clip : 0.f;   // a candidate the delta path could not serve teaches nothing
     if (kk.diam != INT_MAX) {
       lab = (float)((double)(kk.total - s->prev_total) * (double)s->label_scale);
       lab = fminf(fmaxf(lab, -s->label_clip), s->label_clip);
@@ -306,10 +287,10 @@ __global__ void decide_kernel(State* __restrict__ s, const Swap* __restrict__ sw
       use_comp = true;
     }
   }
-  for (int c = 0; c < C; ++c) {
+  for (int c = 0; c < C && comp_out; ++c) {
     const int m = pred_size(s->n_pred, c);
     if (m < 1) break;
-    const Key kp = key_of(out[K + c], N);
+    const Key kp = key_of(comp_out[1 + c], N);
     if (key_less(kp, cand)) {
       cand = kp;
       use_comp = false;
@@ -390,63 +371,24 @@ __global__ void best_copy_kernel(const State* __restrict__ s) {
 }
 
 // ---- learned mode: features and selection ---------------------------------------------
-constexpr int kMaxFeatDegree = 16;
+constexpr int kMaxFeatDegree = 32;
 
-// Distance between x and y resolved up to 5 (5 meaning >= 5): y in N(x),
-// N(x) meets N(y), N(x) meets N2(y), N2(x) meets N2(y), where N2(v) lists
-// the neighbours of v's neighbours (d^2 entries, kept in local memory).
-__device__ int joined_distance(const int* __restrict__ A, int d, int x, int y) {
+// Exact distance d(x, y) read from the base: the first level k whose row x
+// (in the window holding source y) has y's bit, i.e. y in S_k[x].  Window
+// completion bounds the search; a stalled window gives level_cap + 1.
+__device__ int base_distance(const uint4* __restrict__ levels, const int* __restrict__ win_levels, int cap, int N,
+                             int x, int y) {
   if (x == y) return 0;
-  const int* rx = A + (long long)x * d;
-  const int* ry = A + (long long)y * d;
-  for (int j = 0; j < d; ++j)
-    if (rx[j] == y) return 1;
-  int n2y[kMaxFeatDegree * kMaxFeatDegree];
-  int m = 0;
-  for (int j = 0; j < d; ++j) {
-    const int* ru = A + (long long)ry[j] * d;
-    for (int q = 0; q < d; ++q) n2y[m++] = ru[q];
+  const int w = y >> 7, b = y & 127;
+  const int L = win_levels[w];
+  const int top = L > 0 ? L : cap;
+  const uint4* lev = levels + (size_t)w * (cap + 1) * N + x;
+  for (int k = 1; k <= top; ++k) {
+    const uint4 r = __ldg(lev + (size_t)k * N);
+    const unsigned wd = b < 64 ? (b < 32 ? r.x : r.y) : (b < 96 ? r.z : r.w);
+    if ((wd >> (b & 31)) & 1u) return k;
   }
-  for (int i = 0; i < d; ++i)
-    for (int j = 0; j < d; ++j)
-      if (rx[i] == ry[j]) return 2;
-  for (int i = 0; i < d; ++i)
-    for (int j = 0; j < m; ++j)
-      if (rx[i] == n2y[j]) return 3;
-  for (int i = 0; i < d; ++i) {
-    const int* ru = A + (long long)rx[i] * d;
-    for (int q = 0; q < d; ++q) {
-      const int w = ru[q];
-      for (int j = 0; j < m; ++j)
-        if (w == n2y[j]) return 4;
-    }
-  }
-  return 5;
-}
-
-__device__ int capped_distance(const int* __restrict__ A, int d, int x, int y) {
-  if (x == y) return 0;
-  const int* rx = A + (long long)x * d;
-  const int* ry = A + (long long)y * d;
-  int ny[kMaxFeatDegree];
-  for (int j = 0; j < d; ++j) ny[j] = ry[j];
-  for (int j = 0; j < d; ++j)
-    if (rx[j] == y) return 1;
-  bool two = false;
-  for (int i = 0; i < d && !two; ++i) {
-    const int u = rx[i];
-    for (int j = 0; j < d; ++j) two |= (ny[j] == u);
-  }
-  if (two) return 2;
-  for (int i = 0; i < d; ++i) {
-    const int* ru = A + (long long)rx[i] * d;
-    for (int q = 0; q < d; ++q) {
-      const int w = ru[q];
-      for (int j = 0; j < d; ++j)
-        if (ny[j] == w) return 3;
-    }
-  }
-  return 4;
+  return cap + 1;
 }
 
 __device__ int common_neighbours(const int* __restrict__ A, int d, int x, int y) {
@@ -462,13 +404,14 @@ __device__ int common_neighbours(const int* __restrict__ A, int d, int x, int y)
 
 // 32 features per candidate, from the current graph's profile (stats) and
 // adjacency: per endpoint (6 each) eccentricity / 8, mean distance / 8 and
-// log-scaled counts of vertices at distance 2..5; the distances of the
-// pairs the swap joins (1..4 or >= 5) and of the two cross pairs (1..3 or
-// >= 4);
+// log-scaled counts of vertices at distance 2..5; the exact distances (read
+// from the base's level rows) of the pairs the swap joins and of the two
+// cross pairs, / 8;
 // the common-neighbour counts of the pairs it separates; and the
 // transmission gaps of the joined pairs.
 __global__ void features_kernel(const State* __restrict__ s, const Swap* __restrict__ sw, int G,
-                                const unsigned* __restrict__ stats, bf16* __restrict__ X) {
+                                const unsigned* __restrict__ stats, const uint4* __restrict__ levels,
+                                const int* __restrict__ win_levels, int cap, bf16* __restrict__ X) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= G) return;
   float f[mlp::kFeatures];
@@ -498,10 +441,10 @@ __global__ void features_kernel(const State* __restrict__ s, const Swap* __restr
       }
     }
     const int* A = s->adj;
-    f[24] = joined_distance(A, d, w.x[0], w.x[2]) * 0.2f;
-    f[25] = joined_distance(A, d, w.x[1], w.x[3]) * 0.2f;
-    f[26] = capped_distance(A, d, w.x[0], w.x[3]) * 0.25f;
-    f[27] = capped_distance(A, d, w.x[1], w.x[2]) * 0.25f;
+    f[24] = base_distance(levels, win_levels, cap, N, w.x[0], w.x[2]) * 0.125f;
+    f[25] = base_distance(levels, win_levels, cap, N, w.x[1], w.x[3]) * 0.125f;
+    f[26] = base_distance(levels, win_levels, cap, N, w.x[0], w.x[3]) * 0.125f;
+    f[27] = base_distance(levels, win_levels, cap, N, w.x[1], w.x[2]) * 0.125f;
     f[28] = (float)common_neighbours(A, d, w.x[0], w.x[1]) / (float)d;
     f[29] = (float)common_neighbours(A, d, w.x[2], w.x[3]) / (float)d;
     f[30] = fabsf(T[0] - T[2]) / (float)(N - 1);
@@ -588,23 +531,26 @@ __global__ void pred_list_kernel(State* __restrict__ s, const Swap* __restrict__
   s->n_pred = m;
 }
 
-// Slots K .. K+C-1: the current adjacency (blockIdx.y = composite), then
-// patch_pred_kernel applies each composite's swaps.
-__global__ void copy_pred_kernel(const State* __restrict__ s, int* __restrict__ slots, long long slot_stride, int K) {
+// The composite batch: slot 0 the exact composite, slot 1 + c predicted
+// composite c.  Every slot first gets the current adjacency (blockIdx.y =
+// slot), then patch_composites_kernel applies each slot's swaps.
+__global__ void copy_composites_kernel(const State* __restrict__ s, int* __restrict__ slots, long long slot_stride) {
   if (s->done) return;
   const long long n = (long long)s->N * s->d;
-  int* dst = slots + (long long)(K + blockIdx.y) * slot_stride;
+  int* dst = slots + (long long)blockIdx.y * slot_stride;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
     dst[i] = s->adj[i];
 }
 
-__global__ void patch_pred_kernel(const State* __restrict__ s, const Swap* __restrict__ pred, int* __restrict__ slots,
-                                  long long slot_stride, int K) {
+__global__ void patch_composites_kernel(const State* __restrict__ s, const Swap* __restrict__ comp,
+                                        const Swap* __restrict__ pred, int* __restrict__ slots,
+                                        long long slot_stride) {
   if (s->done) return;
-  const int c = blockIdx.x;
-  int* dst = slots + (long long)(K + c) * slot_stride;
-  const int m = pred_size(s->n_pred, c);
-  for (int i = threadIdx.x; i < m; i += blockDim.x) apply_swap(dst, s->d, pred[i]);
+  const int slot = blockIdx.x;
+  int* dst = slots + (long long)slot * slot_stride;
+  const Swap* list = slot == 0 ? comp : pred;
+  const int m = slot == 0 ? s->n_comp : pred_size(s->n_pred, slot - 1);
+  for (int i = threadIdx.x; i < m; i += blockDim.x) apply_swap(dst, s->d, list[i]);
 }
 
 }  // namespace sa
@@ -620,30 +566,45 @@ struct ggb_sa {
   int K = 0, G = 0, n_rand = 0, compose_max = 0;
   int C = 0, pred_max = 0;        // predicted composites (learned mode) and their largest size
   bool learned = false;
+  bool delta = false;             // candidates evaluated against the base, not in full
   State h{};                      // host mirror of the device state
   State* d_state = nullptr;
   int* d_edges = nullptr;
   int* d_adj = nullptr;
   int* d_best_edges = nullptr;
-  Swap* d_swaps = nullptr;        // [G]
+  Swap* d_swaps = nullptr;        // [max(G, K)]
   int* d_sel = nullptr;           // [K]
   Swap* d_comp = nullptr;         // [compose_max]
+  Swap* d_pred = nullptr;         // [pred_max]
   unsigned* d_vmark = nullptr;    // [N/32 + 1]
   float* d_labels = nullptr;      // [K]
-  float* d_scores = nullptr;      // [G]
-  __nv_bfloat16* d_X = nullptr;   // [G][32]
-  unsigned* d_stats = nullptr;    // [N][kStatLevels]
-  int* d_sticky = nullptr;        // first device error of any evaluation in a step
-  ggb_batch* cand = nullptr;      // K candidates, then C predicted composites
+  float* d_scores = nullptr;      // [max(G, K)]
   int* d_rank = nullptr;          // [G] ranking of the proposals
   float* d_rank_key = nullptr;    // [G]
-  Swap* d_pred = nullptr;         // [pred_max]
-  ggb_batch* comp = nullptr;      // the composite
+  __nv_bfloat16* d_X = nullptr;   // [max(G, K)][32]
+  unsigned* d_stats = nullptr;    // [N][kStatLevels]
+  int* d_sticky = nullptr;        // first device error of any evaluation in a step
+  ggb_batch* cand = nullptr;      // full mode: the K candidates
+  ggb_batch* comp = nullptr;      // slot 0: exact composite; slot 1 + c: predicted composite c
   ggb_mlp* mlp = nullptr;
-  // profile launch
+  // profile launch (learned mode without delta)
   int pR = 0;
   ggb::ApspCtrl* d_pctrl = nullptr;
   uint4* d_pbuf = nullptr;
+  // the base (delta mode): R = 1 windows of the current graph, all levels kept
+  int nwin = 0, level_cap = 0, base_T = 0, base_teams = 0;
+  uint4* d_levels = nullptr;
+  long long* d_lcounts = nullptr;
+  int* d_winlev = nullptr;
+  ggb::ApspCtrl* d_bctrl = nullptr;   // [0]: the grid barrier, [1 + t]: team t
+  uint4* d_bscratch = nullptr;
+  ggb::BaseResult* d_bres = nullptr;
+  long long* d_dsum = nullptr;        // [K][nwin]
+  int* d_dlev = nullptr;              // [K][nwin]
+  ggb::BatchOut* d_dout = nullptr;    // [K]
+  uint4* d_dpool = nullptr;           // dense fallback slots of the delta evaluation
+  int* d_dused = nullptr;
+  int dense_slots = 0;
   cudaStream_t st = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
@@ -679,40 +640,106 @@ size_t profile_smem_for(int R) {
   }
 }
 
-int enqueue_profile(ggb_sa* a, const int* gate, cudaStream_t st) {
-  SCUDA(cudaMemsetAsync(a->d_pctrl, 0, sizeof(ggb::ApspCtrl), st));
+ggb::ApspArgs graph_args(ggb_sa* a) {
   ggb::ApspArgs p;
   std::memset(&p, 0, sizeof p);
   p.adj = a->d_adj;
-  p.adj2 = nullptr;
-  p.buf0 = a->d_pbuf;
-  p.buf1 = a->d_pbuf + (size_t)a->N * a->pR;
-  p.ctrl = a->d_pctrl;
   p.timeout_ns = 2000000000LL;
   p.N = a->N;
   p.d = a->d;
   p.n_src1 = a->N;
   p.split = a->N;
-  p.ac = 0;
   p.groups = 1;
   p.win_first = 0;
   p.win_stride = 1;
   p.vec4 = (a->d % 4 == 0) ? 1 : 0;
-  p.stats = a->d_stats;
+  return p;
+}
+
+int coop_launch(const void* fn, int grid, size_t smem, void** params, cudaStream_t st) {
   cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(a->sms);
+  cfg.gridDim = dim3(grid);
   cfg.blockDim = dim3(ggb::kThreads);
-  cfg.dynamicSmemBytes = profile_smem_for(a->pR);
+  cfg.dynamicSmemBytes = smem;
   cfg.stream = st;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeCooperative;
   attr[0].val.cooperative = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
+  SCUDA(cudaLaunchKernelExC(&cfg, fn, params));
+  ggb::core_add_launches(1);
+  return GGB_OK;
+}
+
+// Profile of the current graph (per-vertex statistics), gated on *gate.
+int enqueue_profile(ggb_sa* a, const int* gate, cudaStream_t st) {
+  SCUDA(cudaMemsetAsync(a->d_pctrl, 0, sizeof(ggb::ApspCtrl), st));
+  ggb::ApspArgs p = graph_args(a);
+  p.buf0 = a->d_pbuf;
+  p.buf1 = a->d_pbuf + (size_t)a->N * a->pR;
+  p.ctrl = a->d_pctrl;
+  p.stats = a->d_stats;
   int* sticky = a->d_sticky;
   void* params[] = {(void*)&p, (void*)&gate, (void*)&sticky};
-  SCUDA(cudaLaunchKernelExC(&cfg, profile_kernel_for(a->pR), params));
-  ggb::core_add_launches(1);
+  return coop_launch(profile_kernel_for(a->pR), a->sms, profile_smem_for(a->pR), params, st);
+}
+
+// The base of the delta evaluation (and, with a filter, the statistics),
+// gated on *gate.
+int enqueue_base(ggb_sa* a, const int* gate, cudaStream_t st) {
+  SCUDA(cudaMemsetAsync(a->d_bctrl, 0, (size_t)(1 + a->base_teams) * sizeof(ggb::ApspCtrl), st));
+  ggb::ApspArgs p = graph_args(a);
+  p.stats = a->learned ? a->d_stats : nullptr;
+  p.levels = a->d_levels;
+  p.level_counts = a->d_lcounts;
+  p.win_levels = a->d_winlev;
+  p.level_cap = a->level_cap;
+  ggb::BaseArgs b;
+  b.grid_ctrl = a->d_bctrl;
+  b.team_ctrl = a->d_bctrl + 1;
+  b.scratch = a->d_bscratch;
+  b.result = a->d_bres;
+  b.gate = gate;
+  b.sticky = a->d_sticky;
+  b.n_teams = a->base_teams;
+  b.team_ctas = a->base_T;
+  void* params[] = {(void*)&p, (void*)&b};
+  return coop_launch((const void*)ggb::apsp_base_kernel<1>, a->base_teams * a->base_T, ggb::apsp_smem_bytes<1>(),
+                     params, st);
+}
+
+ggb::DeltaArgs delta_args(ggb_sa* a, const int* sel) {
+  ggb::DeltaArgs g;
+  g.levels = a->d_levels;
+  g.level_counts = a->d_lcounts;
+  g.win_levels = a->d_winlev;
+  g.adj = a->d_adj;
+  g.sw = a->d_swaps;
+  g.sel = sel;
+  g.stop = &a->d_state->done;
+  g.dsum = a->d_dsum;
+  g.dlev = a->d_dlev;
+  g.dense_pool = a->d_dpool;
+  g.dense_used = a->d_dused;
+  g.dense_slots = a->dense_slots;
+  g.N = a->N;
+  g.d = a->d;
+  g.nwin = a->nwin;
+  g.n_src = a->N;
+  g.level_cap = a->level_cap;
+  g.K = a->K;
+  return g;
+}
+
+int enqueue_delta(ggb_sa* a, const int* sel, cudaStream_t st) {
+  const ggb::DeltaArgs g = delta_args(a, sel);
+  const size_t smem = (size_t)((a->N + 31) / 32) * sizeof(unsigned);
+  SCUDA(cudaMemsetAsync(a->d_dused, 0, sizeof(int), st));
+  ggb::delta_kernel<<<a->K * a->nwin, ggb::kDeltaThreads, smem, st>>>(g);
+  ggb::delta_reduce_kernel<<<(a->K + 7) / 8, 256, 0, st>>>(g, a->d_bres, a->d_dout);
+  ggb::core_add_launches(2);
+  SCUDA(cudaGetLastError());
   return GGB_OK;
 }
 
@@ -725,7 +752,8 @@ int enqueue_step(ggb_sa* a, cudaStream_t st) {
   int launches = 1;
   const int* sel = nullptr;
   if (a->learned) {
-    features_kernel<<<(G + 127) / 128, 128, 0, st>>>(s, a->d_swaps, G, a->d_stats, a->d_X);
+    features_kernel<<<(G + 127) / 128, 128, 0, st>>>(s, a->d_swaps, G, a->d_stats, a->d_levels, a->d_winlev,
+                                                     a->level_cap, a->d_X);
     int rc = ggb::mlp_forward(a->mlp, a->d_X, G, a->d_scores, st, false);
     if (rc) return rc;
     select_kernel<<<1, 1024, 0, st>>>(s, a->d_swaps, a->d_scores, G, a->K, a->n_rand, a->d_sel, a->d_rank,
@@ -733,38 +761,53 @@ int enqueue_step(ggb_sa* a, cudaStream_t st) {
     sel = a->d_sel;
     launches += 2;
   }
-  const long long stride = a->cand->off.size() > 1 ? a->cand->off[1] - a->cand->off[0] : 0;
-  const int bx = std::max(1, std::min(a->sms * 4 / std::max(a->K, 1), (int)(((long long)a->N * a->d + 255) / 256)));
-  materialize_kernel<<<dim3(bx, a->K), 256, 0, st>>>(s, a->d_swaps, sel, a->cand->d_adj, stride);
-  if (a->C > 0) {
-    pred_list_kernel<<<1, 32, 0, st>>>(s, a->d_swaps, a->d_rank, a->d_rank_key, G, a->pred_max, a->d_pred,
-                                       a->d_vmark);
-    copy_pred_kernel<<<dim3(bx, a->C), 256, 0, st>>>(s, a->cand->d_adj, stride, a->K);
-    patch_pred_kernel<<<a->C, 128, 0, st>>>(s, a->d_pred, a->cand->d_adj, stride, a->K);
-    launches += 3;
+  int rc;
+  const ggb::BatchOut* singles;
+  if (a->delta) {
+    rc = enqueue_delta(a, sel, st);
+    if (rc) return rc;
+    singles = a->d_dout;
+  } else {
+    const long long stride = a->cand->off.size() > 1 ? a->cand->off[1] - a->cand->off[0] : 0;
+    const int bx = std::max(1, std::min(a->sms * 4 / std::max(a->K, 1), (int)(((long long)a->N * a->d + 255) / 256)));
+    materialize_kernel<<<dim3(bx, a->K), 256, 0, st>>>(s, a->d_swaps, sel, a->cand->d_adj, stride);
+    rc = ggb::batch_enqueue(a->cand, st);
+    if (rc) return rc;
+    singles = a->cand->d_out;
+    launches += 1;
   }
-  int rc = ggb::batch_enqueue(a->cand, st);
-  if (rc) return rc;
-  compose_kernel<<<1, kComposeThreads, 0, st>>>(s, a->d_swaps, sel, a->cand->d_out, a->K, a->d_comp,
-                                                a->compose_max, a->d_vmark);
-  launches += 3;
+  compose_kernel<<<1, kComposeThreads, 0, st>>>(s, a->d_swaps, sel, singles, a->K, a->d_comp, a->compose_max,
+                                                a->d_vmark);
+  launches += 1;
   const ggb::BatchOut* comp_out = nullptr;
-  if (a->compose_max >= 2) {
-    copy_current_kernel<<<a->sms, 256, 0, st>>>(s, a->comp->d_adj);
-    patch_composite_kernel<<<1, 128, 0, st>>>(s, a->d_comp, a->comp->d_adj);
+  if (a->comp) {
+    if (a->C > 0) {
+      pred_list_kernel<<<1, 32, 0, st>>>(s, a->d_swaps, a->d_rank, a->d_rank_key, G, a->pred_max, a->d_pred,
+                                         a->d_vmark);
+      launches += 1;
+    }
+    const long long stride = a->comp->off.size() > 1 ? a->comp->off[1] - a->comp->off[0] : 0;
+    const int slots = 1 + a->C;
+    const int bx = std::max(1, std::min(a->sms * 4 / slots, (int)(((long long)a->N * a->d + 255) / 256)));
+    copy_composites_kernel<<<dim3(bx, slots), 256, 0, st>>>(s, a->comp->d_adj, stride);
+    patch_composites_kernel<<<slots, 128, 0, st>>>(s, a->d_comp, a->d_pred, a->comp->d_adj, stride);
     rc = ggb::batch_enqueue(a->comp, st);
     if (rc) return rc;
     comp_out = a->comp->d_out;
-    launches += 3;
+    launches += 2;
   }
-  decide_kernel<<<1, std::max(32, (a->K + 31) / 32 * 32), 0, st>>>(s, a->d_swaps, sel, a->cand->d_out, a->K,
-                                                                   a->d_comp, comp_out,
-                                                                   a->learned ? a->d_labels : nullptr, a->d_pred,
-                                                                   a->C);
+  decide_kernel<<<1, std::max(32, (a->K + 31) / 32 * 32), 0, st>>>(s, a->d_swaps, sel, singles, a->K, a->d_comp,
+                                                                   comp_out, a->learned ? a->d_labels : nullptr,
+                                                                   a->d_pred, a->comp ? a->C : 0);
   launches += 1;
   if (a->learned) {
     rc = ggb::mlp_train_rows(a->mlp, a->d_X, a->d_sel, a->d_labels, a->K, st);
     if (rc) return rc;
+  }
+  if (a->delta) {
+    rc = enqueue_base(a, &s->accepted, st);
+    if (rc) return rc;
+  } else if (a->learned) {
     rc = enqueue_profile(a, &s->accepted, st);
     if (rc) return rc;
   }
@@ -794,6 +837,13 @@ int capture_step(ggb_sa* a) {
   return GGB_OK;
 }
 
+void drop_graph(ggb_sa* a) {
+  if (a->exec) cudaGraphExecDestroy(a->exec);
+  if (a->graph) cudaGraphDestroy(a->graph);
+  a->exec = nullptr;
+  a->graph = nullptr;
+}
+
 int pull_state(ggb_sa* a) {
   SCUDA(cudaMemcpyAsync(&a->h, a->d_state, sizeof(State), cudaMemcpyDeviceToHost, a->st));
   SCUDA(cudaStreamSynchronize(a->st));
@@ -810,12 +860,13 @@ void destroy(ggb_sa* a) {
   if (!a) return;
   if (a->device >= 0) cudaSetDevice(a->device);
   if (a->st) cudaStreamSynchronize(a->st);
-  if (a->exec) cudaGraphExecDestroy(a->exec);
-  if (a->graph) cudaGraphDestroy(a->graph);
+  drop_graph(a);
   for (void* q : {(void*)a->d_state, (void*)a->d_edges, (void*)a->d_adj, (void*)a->d_best_edges, (void*)a->d_swaps,
-                  (void*)a->d_sel, (void*)a->d_comp, (void*)a->d_vmark, (void*)a->d_labels, (void*)a->d_scores,
-                  (void*)a->d_X, (void*)a->d_stats, (void*)a->d_pctrl, (void*)a->d_pbuf, (void*)a->d_sticky,
-                  (void*)a->d_rank, (void*)a->d_rank_key, (void*)a->d_pred})
+                  (void*)a->d_sel, (void*)a->d_comp, (void*)a->d_pred, (void*)a->d_vmark, (void*)a->d_labels,
+                  (void*)a->d_scores, (void*)a->d_rank, (void*)a->d_rank_key, (void*)a->d_X, (void*)a->d_stats,
+                  (void*)a->d_sticky, (void*)a->d_pctrl, (void*)a->d_pbuf, (void*)a->d_levels, (void*)a->d_lcounts,
+                  (void*)a->d_winlev, (void*)a->d_bctrl, (void*)a->d_bscratch, (void*)a->d_bres, (void*)a->d_dsum,
+                  (void*)a->d_dlev, (void*)a->d_dout, (void*)a->d_dpool, (void*)a->d_dused})
     cudaFree(q);
   if (a->cand) ggb_batch_destroy(a->cand);
   if (a->comp) ggb_batch_destroy(a->comp);
@@ -825,20 +876,72 @@ void destroy(ggb_sa* a) {
   delete a;
 }
 
-// Evaluates the current graph exactly (profile kernel, ungated) and sets the
-// current and best values from it.
+int check_sticky(ggb_sa* a) {
+  int sticky = 0;
+  SCUDA(cudaMemcpy(&sticky, a->d_sticky, sizeof sticky, cudaMemcpyDeviceToHost));
+  if (sticky == ggb::kErrTimeout) return core_fail(GGB_ETIMEOUT, "a barrier wait of an annealing step ran out");
+  if (sticky == ggb::kErrAdj) return core_fail(GGB_EADJ, "an annealing candidate had an entry outside [0, nodes)");
+  if (sticky) return core_fail(GGB_ECUDA, "an annealing evaluation failed (device error %d)", sticky);
+  return GGB_OK;
+}
+
+// Evaluates the current graph exactly (ungated base build or profile) and
+// sets the current and best values from it.
 int evaluate_current(ggb_sa* a) {
-  int rc = enqueue_profile(a, nullptr, a->st);
-  if (rc) return rc;
-  ggb::ApspCtrl c;
-  SCUDA(cudaMemcpyAsync(&c, a->d_pctrl, sizeof c, cudaMemcpyDeviceToHost, a->st));
-  SCUDA(cudaStreamSynchronize(a->st));
-  if (c.error == ggb::kErrAdj) return core_fail(GGB_EADJ, "edge list has an endpoint outside [0, nodes)");
-  if (c.error) return core_fail(GGB_ECUDA, "profile evaluation failed (device error %d)", c.error);
-  if (!c.done) return core_fail(GGB_ECUDA, "profile evaluation did not complete");
-  if (c.disconnected || c.diam >= a->N) return core_fail(GGB_EINVAL, "the initial graph is not connected");
-  a->h.cur_diam = a->h.best_diam = c.diam;
-  a->h.cur_total = a->h.best_total = a->h.prev_total = c.sum + (long long)a->N * (a->N - 1);
+  long long sum = 0;
+  int diam = 0, disc = 0;
+  if (a->delta) {
+    int rc = enqueue_base(a, nullptr, a->st);
+    if (rc) return rc;
+    ggb::BaseResult r;
+    SCUDA(cudaMemcpyAsync(&r, a->d_bres, sizeof r, cudaMemcpyDeviceToHost, a->st));
+    SCUDA(cudaStreamSynchronize(a->st));
+    rc = check_sticky(a);
+    if (rc) return rc;
+    sum = r.sum;
+    diam = r.diam;
+    disc = r.disconnected;
+  } else {
+    int rc = enqueue_profile(a, nullptr, a->st);
+    if (rc) return rc;
+    ggb::ApspCtrl c;
+    SCUDA(cudaMemcpyAsync(&c, a->d_pctrl, sizeof c, cudaMemcpyDeviceToHost, a->st));
+    SCUDA(cudaStreamSynchronize(a->st));
+    rc = check_sticky(a);
+    if (rc) return rc;
+    if (!c.done) return core_fail(GGB_ECUDA, "profile evaluation did not complete");
+    sum = c.sum;
+    diam = c.diam;
+    disc = c.disconnected;
+  }
+  if (disc || diam >= a->N) return core_fail(GGB_EINVAL, "the initial graph is not connected");
+  a->h.cur_diam = a->h.best_diam = diam;
+  a->h.cur_total = a->h.best_total = a->h.prev_total = sum + (long long)a->N * (a->N - 1);
+  return GGB_OK;
+}
+
+int alloc_base(ggb_sa* a) {
+  a->nwin = (a->N + 127) / 128;
+  a->level_cap = 15;
+  a->base_T = 4;
+  a->base_teams = std::max(1, std::min(a->sms / a->base_T, a->nwin));
+  int nb = 0;
+  SCUDA(cudaFuncSetAttribute((const void*)ggb::apsp_base_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)ggb::apsp_smem_bytes<1>()));
+  SCUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, (const void*)ggb::apsp_base_kernel<1>, ggb::kThreads,
+                                                      ggb::apsp_smem_bytes<1>()));
+  if (nb < 1) return core_fail(GGB_ECUDA, "base kernel cannot be resident");
+  const size_t cells = (size_t)a->nwin * (a->level_cap + 1) * a->N;
+  int rc;
+  if ((rc = sdev(&a->d_levels, cells)) || (rc = sdev(&a->d_lcounts, (size_t)a->nwin * (a->level_cap + 1))) ||
+      (rc = sdev(&a->d_winlev, (size_t)a->nwin)) || (rc = sdev(&a->d_bctrl, (size_t)1 + a->base_teams)) ||
+      (rc = sdev(&a->d_bscratch, (size_t)a->base_teams * 2 * a->N)) || (rc = sdev(&a->d_bres, 1)) ||
+      (rc = sdev(&a->d_dsum, (size_t)a->K * a->nwin)) || (rc = sdev(&a->d_dlev, (size_t)a->K * a->nwin)) ||
+      (rc = sdev(&a->d_dout, (size_t)a->K)))
+    return rc;
+  // dense fallback: up to 8 windows per candidate, at most 1 GiB
+  a->dense_slots = (int)std::max<long long>(1, std::min<long long>(8LL * a->K, (1LL << 30) / (32LL * a->N)));
+  if ((rc = sdev(&a->d_dpool, (size_t)a->dense_slots * 2 * a->N)) || (rc = sdev(&a->d_dused, 1))) return rc;
   return GGB_OK;
 }
 
@@ -851,6 +954,7 @@ int create(ggb_sa* a, int nodes, int degree, const int* edges, int K, int G, int
   a->K = K;
   a->G = G;
   a->learned = G > K;
+  a->delta = K > 1;
   a->compose_max = compose_max;
   a->n_rand = a->learned ? std::max(1, K / 4) : 0;
   a->C = a->learned ? 4 : 0;
@@ -876,23 +980,23 @@ int create(ggb_sa* a, int nodes, int degree, const int* edges, int K, int G, int
   }
   int rc;
   const size_t L2 = (size_t)2 * a->lines;
+  const size_t GK = (size_t)std::max(G, K);
   if ((rc = sdev(&a->d_state, 1)) || (rc = sdev(&a->d_edges, L2)) || (rc = sdev(&a->d_adj, adj.size())) ||
-      (rc = sdev(&a->d_best_edges, L2)) || (rc = sdev(&a->d_swaps, (size_t)std::max(G, K))) ||
-      (rc = sdev(&a->d_sel, (size_t)K)) || (rc = sdev(&a->d_comp, (size_t)std::max(compose_max, 1))) ||
+      (rc = sdev(&a->d_best_edges, L2)) || (rc = sdev(&a->d_swaps, GK)) || (rc = sdev(&a->d_sel, (size_t)K)) ||
+      (rc = sdev(&a->d_comp, (size_t)std::max(compose_max, 1))) ||
+      (rc = sdev(&a->d_pred, (size_t)std::max(a->pred_max, 1))) ||
       (rc = sdev(&a->d_vmark, (size_t)nodes / 32 + 1)) || (rc = sdev(&a->d_labels, (size_t)K)) ||
-      (rc = sdev(&a->d_scores, (size_t)std::max(G, K))) ||
-      (rc = sdev(&a->d_X, (size_t)std::max(G, K) * ggb::mlp::kFeatures)) ||
-      (rc = sdev(&a->d_stats, (size_t)nodes * ggb::kStatLevels)) || (rc = sdev(&a->d_pctrl, 1)) ||
-      (rc = sdev(&a->d_sticky, 1)) || (rc = sdev(&a->d_rank, (size_t)std::max(G, K))) ||
-      (rc = sdev(&a->d_rank_key, (size_t)std::max(G, K))) || (rc = sdev(&a->d_pred, (size_t)std::max(a->pred_max, 1))))
+      (rc = sdev(&a->d_scores, GK)) || (rc = sdev(&a->d_rank, GK)) || (rc = sdev(&a->d_rank_key, GK)) ||
+      (rc = sdev(&a->d_X, GK * ggb::mlp::kFeatures)) || (rc = sdev(&a->d_stats, (size_t)nodes * ggb::kStatLevels)) ||
+      (rc = sdev(&a->d_pctrl, 1)) || (rc = sdev(&a->d_sticky, 1)))
     return rc;
   SCUDA(cudaMemset(a->d_sticky, 0, sizeof(int)));
   SCUDA(cudaMemcpy(a->d_edges, edges, L2 * sizeof(int), cudaMemcpyHostToDevice));
   SCUDA(cudaMemcpy(a->d_best_edges, edges, L2 * sizeof(int), cudaMemcpyHostToDevice));
   SCUDA(cudaMemcpy(a->d_adj, adj.data(), adj.size() * sizeof(int), cudaMemcpyHostToDevice));
   SCUDA(cudaMemset(a->d_vmark, 0, ((size_t)nodes / 32 + 1) * sizeof(unsigned)));
-  SCUDA(cudaMemset(a->d_swaps, 0, (size_t)std::max(G, K) * sizeof(Swap)));
-  SCUDA(cudaMemset(a->d_X, 0, (size_t)std::max(G, K) * ggb::mlp::kFeatures * sizeof(__nv_bfloat16)));
+  SCUDA(cudaMemset(a->d_swaps, 0, GK * sizeof(Swap)));
+  SCUDA(cudaMemset(a->d_X, 0, GK * ggb::mlp::kFeatures * sizeof(__nv_bfloat16)));
   // profile window: the widest of 2048 / 4096 / 8192 sources whose two matrices fit in about half the L2
   a->pR = 16;
   for (int R = 64; R >= 16; R /= 2)
@@ -906,20 +1010,23 @@ int create(ggb_sa* a, int nodes, int degree, const int* edges, int K, int G, int
     if (nb < 1) return core_fail(GGB_ECUDA, "profile kernel R=%d cannot be resident", R);
   }
   if ((rc = sdev(&a->d_pbuf, (size_t)2 * nodes * a->pR))) return rc;
-  // the candidate batch and the composite
-  const int nb = K + a->C;
-  std::vector<int> nn(nb, nodes), bn(nb, nodes), gg(nb, 1), dd(nb, degree);
-  if ((rc = ggb_batch_create(nb, nn.data(), bn.data(), gg.data(), dd.data(), &a->cand))) return rc;
-  a->cand->stop = &a->d_state->done;
-  a->cand->sticky = a->d_sticky;
-  if (compose_max >= 2) {
-    if ((rc = ggb_batch_create(1, nn.data(), bn.data(), gg.data(), dd.data(), &a->comp))) return rc;
+  if (a->delta && (rc = alloc_base(a))) return rc;
+  // the candidate batch (full mode) and the composite batch
+  const int nc = 1 + a->C;
+  const int nmax = std::max(K, nc);
+  std::vector<int> nn(nmax, nodes), bn(nmax, nodes), gg(nmax, 1), dd(nmax, degree);
+  if (!a->delta) {
+    if ((rc = ggb_batch_create(K, nn.data(), bn.data(), gg.data(), dd.data(), &a->cand))) return rc;
+    a->cand->stop = &a->d_state->done;
+    a->cand->sticky = a->d_sticky;
+  }
+  if (compose_max >= 2 || a->C > 0) {
+    if ((rc = ggb_batch_create(nc, nn.data(), bn.data(), gg.data(), dd.data(), &a->comp))) return rc;
     a->comp->stop = &a->d_state->done;
     a->comp->sticky = a->d_sticky;
-    if ((rc = ggb_batch_set_plan(a->comp, 0, a->sms))) return rc;
   }
   if (a->learned) {
-    if ((rc = ggb_mlp_create(std::max(G, K), seed ^ 0x4d4c50ULL, &a->mlp))) return rc;
+    if ((rc = ggb_mlp_create((int)GK, seed ^ 0x4d4c50ULL, &a->mlp))) return rc;
   }
   // initial state
   std::memset(&a->h, 0, sizeof a->h);
@@ -941,17 +1048,18 @@ int create(ggb_sa* a, int nodes, int degree, const int* edges, int K, int G, int
   a->h.label_clip = 16.0f;
   if ((rc = push_state(a))) return rc;
   if ((rc = evaluate_current(a))) return rc;
-  if ((rc = push_state(a))) return rc;
-  // candidate slots hold the current graph until the first step
-  for (int k = 0; k < nb; ++k) {
-    int* slot = nullptr;
-    ggb_batch_adj_device(a->cand, k, &slot);
-    SCUDA(cudaMemcpy(slot, a->d_adj, adj.size() * sizeof(int), cudaMemcpyDeviceToDevice));
+  if (a->learned && a->delta) {
+    // the statistics of the features come from the base build, which fills them
   }
-  if (a->comp) {
-    int* cslot = nullptr;
-    ggb_batch_adj_device(a->comp, 0, &cslot);
-    SCUDA(cudaMemcpy(cslot, a->d_adj, adj.size() * sizeof(int), cudaMemcpyDeviceToDevice));
+  if ((rc = push_state(a))) return rc;
+  // batch slots hold the current graph until the first step
+  for (ggb_batch* b : {a->cand, a->comp}) {
+    if (!b) continue;
+    for (int k = 0; k < b->n; ++k) {
+      int* slot = nullptr;
+      ggb_batch_adj_device(b, k, &slot);
+      SCUDA(cudaMemcpy(slot, a->d_adj, adj.size() * sizeof(int), cudaMemcpyDeviceToDevice));
+    }
   }
   return GGB_OK;
 }
@@ -1004,6 +1112,37 @@ int ggb_sa_set_schedule(ggb_sa* a, double temp, double cooling_rate, int hill_cl
   return push_state(a);
 }
 
+int ggb_sa_set_predicted(ggb_sa* a, int composites, int max_swaps) {
+  if (!a) return core_fail(GGB_EINVAL, "null annealer");
+  if (composites < 0 || composites > 8 || max_swaps < 1 || max_swaps > 4096)
+    return core_fail(GGB_EINVAL, "composites in [0, 8] and max_swaps in [1, 4096]");
+  if (composites > 0 && !a->learned) return core_fail(GGB_EPERM, "predicted composites need a proposal filter");
+  SCUDA(cudaSetDevice(a->device));
+  SCUDA(cudaStreamSynchronize(a->st));
+  drop_graph(a);
+  if (a->comp) ggb_batch_destroy(a->comp);
+  a->comp = nullptr;
+  cudaFree(a->d_pred);
+  a->d_pred = nullptr;
+  a->C = composites;
+  a->pred_max = max_swaps;
+  int rc = sdev(&a->d_pred, (size_t)max_swaps);
+  if (rc) return rc;
+  if (a->compose_max >= 2 || a->C > 0) {
+    const int nc = 1 + a->C;
+    std::vector<int> nn(nc, a->N), gg(nc, 1), dd(nc, a->d);
+    if ((rc = ggb_batch_create(nc, nn.data(), nn.data(), gg.data(), dd.data(), &a->comp))) return rc;
+    a->comp->stop = &a->d_state->done;
+    a->comp->sticky = a->d_sticky;
+    for (int k = 0; k < nc; ++k) {
+      int* slot = nullptr;
+      ggb_batch_adj_device(a->comp, k, &slot);
+      SCUDA(cudaMemcpy(slot, a->d_adj, (size_t)a->N * a->d * sizeof(int), cudaMemcpyDeviceToDevice));
+    }
+  }
+  return GGB_OK;
+}
+
 int ggb_sa_set_target(ggb_sa* a, int diameter, long long total) {
   if (!a) return core_fail(GGB_EINVAL, "null annealer");
   SCUDA(cudaSetDevice(a->device));
@@ -1019,13 +1158,15 @@ int ggb_sa_set_target(ggb_sa* a, int diameter, long long total) {
 int ggb_sa_autotune(ggb_sa* a, int iters, int* window_bits, int* team_ctas, double* best_ms) {
   if (!a) return core_fail(GGB_EINVAL, "null annealer");
   SCUDA(cudaSetDevice(a->device));
-  if (a->exec) {
-    cudaGraphExecDestroy(a->exec);
-    cudaGraphDestroy(a->graph);
-    a->exec = nullptr;
-    a->graph = nullptr;
+  drop_graph(a);
+  ggb_batch* b = a->cand ? a->cand : a->comp;
+  if (!b) {
+    if (window_bits) *window_bits = 0;
+    if (team_ctas) *team_ctas = 0;
+    if (best_ms) *best_ms = 0.0;
+    return GGB_OK;
   }
-  return ggb_batch_autotune(a->cand, iters, window_bits, team_ctas, best_ms);
+  return ggb_batch_autotune(b, iters, window_bits, team_ctas, best_ms);
 }
 
 int ggb_sa_run(ggb_sa* a, long long steps, ggb_sa_stats* stats) {
@@ -1035,11 +1176,8 @@ int ggb_sa_run(ggb_sa* a, long long steps, ggb_sa_stats* stats) {
   if (rc) return rc;
   for (long long i = 0; i < steps; ++i) SCUDA(cudaGraphLaunch(a->exec, a->st));
   SCUDA(cudaStreamSynchronize(a->st));
-  int sticky = 0;
-  SCUDA(cudaMemcpy(&sticky, a->d_sticky, sizeof sticky, cudaMemcpyDeviceToHost));
-  if (sticky == ggb::kErrTimeout) return core_fail(GGB_ETIMEOUT, "a barrier wait of an annealing step ran out");
-  if (sticky == ggb::kErrAdj) return core_fail(GGB_EADJ, "an annealing candidate had an entry outside [0, nodes)");
-  if (sticky) return core_fail(GGB_ECUDA, "an annealing evaluation failed (device error %d)", sticky);
+  rc = check_sticky(a);
+  if (rc) return rc;
   rc = pull_state(a);
   if (rc) return rc;
   if (stats) {
@@ -1049,6 +1187,7 @@ int ggb_sa_run(ggb_sa* a, long long steps, ggb_sa_stats* stats) {
     stats->multi_accepts = a->h.multi_accepts;
     stats->moved_swaps = a->h.moved_swaps;
     stats->pred_accepts = a->h.pred_accepts;
+    stats->unevaluated = a->h.unevaluated;
     stats->evals = a->h.evals;
     stats->cur_diam = a->h.cur_diam;
     stats->best_diam = a->h.best_diam;
@@ -1085,12 +1224,56 @@ int ggb_sa_last_step(ggb_sa* a, float* predicted, float* label) {
   return GGB_OK;
 }
 
+int ggb_sa_check_delta(ggb_sa* a, int* compared, int* mismatches, int* unevaluated) {
+  using namespace ggb::sa;
+  if (!a || !compared || !mismatches || !unevaluated) return core_fail(GGB_EINVAL, "null pointer");
+  if (!a->delta) return core_fail(GGB_EPERM, "the annealer does not use the delta evaluation");
+  SCUDA(cudaSetDevice(a->device));
+  int rc = pull_state(a);
+  if (rc) return rc;
+  if (a->h.done) return core_fail(GGB_EPERM, "the annealer has reached its target");
+  // fresh candidates of the current graph, evaluated both ways
+  gen_kernel<<<(a->K + 127) / 128, 128, 0, a->st>>>(a->d_state, a->d_swaps, a->K);
+  rc = enqueue_delta(a, nullptr, a->st);
+  if (rc) return rc;
+  std::vector<int> nn(a->K, a->N), gg1(a->K, 1), dd(a->K, a->d);
+  ggb_batch* full = nullptr;
+  rc = ggb_batch_create(a->K, nn.data(), nn.data(), gg1.data(), dd.data(), &full);
+  if (rc) return rc;
+  const long long stride = full->off.size() > 1 ? full->off[1] - full->off[0] : 0;
+  materialize_kernel<<<dim3(64, a->K), 256, 0, a->st>>>(a->d_state, a->d_swaps, nullptr, full->d_adj, stride);
+  rc = ggb::batch_enqueue(full, a->st);
+  if (!rc) rc = ggb_batch_collect(full, a->st, nullptr);
+  std::vector<ggb::BatchOut> d(a->K);
+  if (!rc && cudaMemcpy(d.data(), a->d_dout, a->K * sizeof(ggb::BatchOut), cudaMemcpyDeviceToHost) != cudaSuccess)
+    rc = core_fail(GGB_ECUDA, "copying the delta results failed");
+  int cmp = 0, bad = 0, unev = 0;
+  if (!rc) {
+    for (int k = 0; k < a->K; ++k) {
+      const ggb::BatchOut& f = full->h_out[k];
+      if (!d[k].done) { ++unev; continue; }
+      ++cmp;
+      const bool fc = !f.disconnected && f.diam < a->N, dc = !d[k].disconnected;
+      if (fc != dc || (fc && (f.diam != d[k].diam || f.sum != d[k].sum))) ++bad;
+    }
+  }
+  ggb_batch_destroy(full);
+  if (rc) return rc;
+  *compared = cmp;
+  *mismatches = bad;
+  *unevaluated = unev;
+  return check_sticky(a);
+}
+
 int ggb_sa_profile(ggb_sa* a, unsigned* stats) {
   if (!a || !stats) return core_fail(GGB_EINVAL, "null pointer");
   SCUDA(cudaSetDevice(a->device));
-  int rc = enqueue_profile(a, nullptr, a->st);
+  // the statistics the features read: from the base build when it makes them
+  int rc = (a->delta && a->learned) ? enqueue_base(a, nullptr, a->st) : enqueue_profile(a, nullptr, a->st);
   if (rc) return rc;
   SCUDA(cudaStreamSynchronize(a->st));
+  rc = check_sticky(a);
+  if (rc) return rc;
   SCUDA(cudaMemcpy(stats, a->d_stats, (size_t)a->N * ggb::kStatLevels * sizeof(unsigned), cudaMemcpyDeviceToHost));
   return GGB_OK;
 }

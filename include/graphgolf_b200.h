@@ -329,6 +329,7 @@ typedef struct ggb_sa ggb_sa;
 typedef struct ggb_sa_stats {
   long long step, accepts, multi_accepts, moved_swaps, evals;
   long long pred_accepts;            /* accepted predicted composites */
+  long long unevaluated;             /* candidates the delta path could not serve (rejected) */
   int cur_diam, best_diam;
   long long cur_total, best_total;   /* exact distance totals (the reference's sum) */
   double cur_aspl, best_aspl;
@@ -338,13 +339,16 @@ typedef struct ggb_sa_stats {
 
 /* edges: [nodes*degree/2][2] (a simple degree-regular graph, connected).
  * candidates in [1, 256]; proposals = candidates (no filter) or a multiple of
- * 16 up to 4096 (then candidates is a multiple of 16, degree <= 16). */
+ * 16 up to 4096 (then candidates is a multiple of 16, degree <= 32). */
 int ggb_sa_create(int nodes, int degree, const int *edges, int candidates, int proposals, int compose_max,
                   unsigned long long seed, ggb_sa **out);
 void ggb_sa_destroy(ggb_sa *a);
 /* Temperature, cooling factor per step, and hill climbing (the reference's
  * -H: accept only when not worse).  Default: hill climbing. */
 int ggb_sa_set_schedule(ggb_sa *a, double temp, double cooling_rate, int hill_climbing);
+/* With a proposal filter: how many predicted composites each step evaluates
+ * (0..8; the default 4) and the largest one's swaps (default 64). */
+int ggb_sa_set_predicted(ggb_sa *a, int composites, int max_swaps);
 /* Stop (every later step does nothing) once diameter <= diameter and the
  * distance total <= total. */
 int ggb_sa_set_target(ggb_sa *a, int diameter, long long total);
@@ -358,6 +362,11 @@ int ggb_sa_edges(ggb_sa *a, int best, int *edges);
  * (scaled change of the distance total) of the last step's `candidates`
  * evaluated swaps; the last quarter of them were drawn at random. */
 int ggb_sa_last_step(ggb_sa *a, float *predicted, float *label);
+/* Self-check of the delta evaluation (candidates > 1): draws `candidates`
+ * fresh swaps of the current graph, evaluates them against the base and in
+ * full, and counts the disagreements in diameter, connectivity or distance
+ * sum among those the delta path served. */
+int ggb_sa_check_delta(ggb_sa *a, int *compared, int *mismatches, int *unevaluated);
 /* Per-vertex level statistics of the current graph, [nodes][32]: entry
  * [v][k] = vertices not within distance k of v. */
 int ggb_sa_profile(ggb_sa *a, unsigned *stats);

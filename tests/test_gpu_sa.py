@@ -41,6 +41,21 @@ def test_hill_climbing_states_exact(gpu, K, G, comp):
         assert st.cur_total < st0.cur_total
 
 
+@pytest.mark.parametrize("n,d,K", [(300, 5, 16), (2048, 12, 64), (5000, 7, 32), (16384, 12, 64)])
+def test_delta_evaluation_exact(gpu, n, d, K):
+    """Candidates evaluated against the base equal their full evaluation,
+    before and after the base is rebuilt by accepted moves."""
+    g = graphs.random_regular(n, d, n + d)
+    with gg.Annealer(g, candidates=K, compose=8, seed=6) as an:
+        total = 0
+        for rounds in range(3):
+            c, m, u = an.check_delta()
+            assert m == 0 and c + u == K and c >= K // 2
+            total += c
+            an.run(3)
+        _check(an, g, an.run(0))
+
+
 def test_metropolis_states_exact(gpu):
     g = graphs.random_regular(400, 5, 4)
     with gg.Annealer(g, candidates=4, seed=9) as an:
