@@ -248,7 +248,11 @@ def main() -> int:
     ap.add_argument("--window-bits", type=int, default=0, help="force the source-window width (0 = automatic)")
     ap.add_argument("--ball", type=int, default=-1, choices=[-1, 0, 1],
                     help="ball pre-pass policy: -1 automatic, 0 never, 1 whenever feasible")
+    ap.add_argument("--case", choices=["sa-step", "batch", "mlp"],
+                    help="run one small case of a component for a profiler and exit")
     args = ap.parse_args()
+    if args.case:
+        return run_case(args.case)
     args.warmup = max(args.warmup, 3)
     wl = WORKLOADS[args.workload]
     if args.impl == "reference":
@@ -504,6 +508,39 @@ def sa_bench(plain_steps: int) -> dict:
                      "final_checked": (r.diameter, r.total) == (s.cur_diam, s.cur_total),
                      "candidates": K, "proposals": G, "speedup_vs_plain": t_plain / el if s.done else None}
     return out
+
+
+def run_case(case: str) -> int:
+    """One small case of a component, for profilers (no JSON line):
+    sa-step  -- 4 steps of the learned annealer, N=16384, d=12, 128 of 4096;
+    batch    -- 2 launches of the mixed batch (4096-bit windows, teams of 16);
+    mlp      -- the filter network: forward of 4096 rows, 2 Adam steps on 128."""
+    import numpy as np
+    import graphgolf_b200 as gg
+    from graphgolf_b200 import graphs
+    lib = gg.load()
+    if lib.ggb_init(0, 0, 0) != 0:
+        raise RuntimeError(gg._native.last_error())
+    if case == "sa-step":
+        a = gg.Annealer(graphs.random_regular(16384, 12, 2), 128, 4096, 128, seed=1)
+        a.predicted(0, 1)
+        st = a.run(4)
+        print("sa-step", st.step, st.accepts, st.cur_total)
+    elif case == "batch":
+        w = graphs.batch_workload()
+        b = gg.Batch([x.nodes for x in w], 12)
+        b.set_plan(4096, 16)
+        b.upload([x.adj for x in w])
+        for _ in range(2):
+            b.launch()
+            r = b.collect()
+        print("batch", b.kernel_ms(), r[0].total)
+    else:
+        net = gg.FilterNet(4096, 1)
+        x = np.random.default_rng(1).uniform(-1, 1, (4096, 32)).astype(np.float32)
+        y = net.forward(x)
+        print("mlp", float(y[0]), net.train(x[:128], 0.5 * y[:128], 2))
+    return 0
 
 
 def reference_cuda(adj, want):

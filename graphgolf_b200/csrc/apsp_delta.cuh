@@ -112,7 +112,7 @@ __global__ void __launch_bounds__(kThreads, 1) apsp_base_kernel(ApspArgs a, cons
   }
 }
 
-// ---- the delta evaluation: one CTA per (candidate, window) -----------------------
+// ---- the delta evaluation: one CTA per (candidate, window), window-major ------------
 constexpr int kDeltaThreads = 256;
 constexpr int kDeltaRows = 512;        // dirty rows a task can hold per level
 constexpr int kDeltaHash = 1024;       // hash slots for the dirty rows (power of two)
@@ -158,7 +158,8 @@ __global__ void __launch_bounds__(kDeltaThreads) delta_kernel(const DeltaArgs a)
   __shared__ int s_over;
   __shared__ unsigned long long s_red[kDeltaThreads / 32];
   if (a.stop && ld_volatile_i32(a.stop) != 0) return;
-  const int c = blockIdx.x / a.nwin, w = blockIdx.x % a.nwin;
+  // window-major: the CTAs resident together share one window's base rows in L2
+  const int c = blockIdx.x % a.K, w = blockIdx.x / a.K;
   const Swap sw = a.sw[a.sel ? a.sel[c] : c];
   const int N = a.N, d = a.d;
   const int base = w * 128;

@@ -189,9 +189,10 @@ __global__ void col_sum_kernel(const float* __restrict__ in, int rows, int cols,
 
 // Adam on the FP32 master parameters, then the BF16 copies the products
 // read (W1, W2 and W2 transposed).  The step counter lives on the device so
-// that a replayed graph keeps counting.  Launched as one block.
+// that a replayed graph keeps counting; adam_step_kernel advances it after
+// every block of this kernel has used it.
 __global__ void adam_kernel(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m1,
-                            float* __restrict__ m2, int* __restrict__ step, AdamHyper h, bf16* __restrict__ w1b,
+                            float* __restrict__ m2, const int* __restrict__ step, AdamHyper h, bf16* __restrict__ w1b,
                             bf16* __restrict__ w2b, bf16* __restrict__ w2tb) {
   const int t = *step + 1;
   const float c1 = 1.f / (1.f - powf(h.beta1, (float)t));
@@ -213,9 +214,9 @@ __global__ void adam_kernel(float* __restrict__ p, const float* __restrict__ g, 
       w2tb[k * kHidden + n] = v;
     }
   }
-  __syncthreads();   // one block: every thread has read *step
-  if (threadIdx.x == 0) *step = t;
 }
+
+__global__ void adam_step_kernel(int* step) { *step += 1; }
 
 // BF16 copies of freshly written FP32 parameters.
 __global__ void cast_params_kernel(const float* __restrict__ p, bf16* __restrict__ w1b, bf16* __restrict__ w2b,
@@ -293,8 +294,10 @@ int mlp_backward(ggb_mlp* m, const bf16* Xs, const float* t, int B, cudaStream_t
 }
 
 int mlp_adam(ggb_mlp* m, cudaStream_t st) {
-  adam_kernel<<<1, 1024, 0, st>>>(m->p, m->g, m->m1, m->m2, m->step, m->hyper, m->W1b, m->W2b, m->W2tb);
-  core_add_launches(1);
+  adam_kernel<<<(kParams + 255) / 256, 256, 0, st>>>(m->p, m->g, m->m1, m->m2, m->step, m->hyper, m->W1b, m->W2b,
+                                                     m->W2tb);
+  adam_step_kernel<<<1, 1, 0, st>>>(m->step);
+  core_add_launches(2);
   MCUDA(cudaGetLastError());
   return GGB_OK;
 }

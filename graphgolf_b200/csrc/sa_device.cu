@@ -205,14 +205,17 @@ __global__ void __launch_bounds__(kComposeThreads) compose_kernel(State* __restr
                                                                   Swap* __restrict__ comp, int compose_max,
                                                                   unsigned* __restrict__ vmark) {
   __shared__ int s_order[kComposeThreads];
+  __shared__ Key s_keys[kComposeThreads];
   if (s->done) return;
   const int N = s->N;
   const int k = threadIdx.x;
+  if (k < K) s_keys[k] = key_of(out[k], N);
+  __syncthreads();
   if (k < K) {
-    const Key me = key_of(out[k], N);
+    const Key me = s_keys[k];
     int rank = 0;
     for (int j = 0; j < K; ++j) {
-      const Key o = key_of(out[j], N);
+      const Key o = s_keys[j];
       rank += key_less(o, me) || (!key_less(me, o) && j < k);
     }
     s_order[rank] = k;
@@ -225,7 +228,7 @@ __global__ void __launch_bounds__(kComposeThreads) compose_kernel(State* __restr
   int m = 0;
   for (int r = 0; r < K && m < compose_max; ++r) {
     const int c = s_order[r];
-    const Key kc = key_of(out[c], N);
+    const Key kc = s_keys[c];
     if (!key_less(kc, cur)) break;   // sorted: nothing further improves
     const Swap w = sw[sel ? sel[c] : c];
     if (!w.valid) continue;
