@@ -112,11 +112,59 @@ __global__ void __launch_bounds__(kThreads, 1) apsp_base_kernel(ApspArgs a, cons
   }
 }
 
+// ---- per-vertex statistics from the kept levels ------------------------------------
+// stats[v][k] = sum over windows of (l - popc(S_k[v])) for k < kStatLevels:
+// the sources not within distance k of v (the statistics the profile
+// kernel accumulates during its sweeps), read back from the base's rows
+// without atomics.  A block takes 32 vertices (one per lane, so loads are
+// coalesced) and its 8 warps split the windows; the partial sums meet in
+// shared memory.  Levels past a window's completion are full and add
+// nothing.  Runs only while *gate != 0.
+constexpr int kStatsWarps = 8;
+__global__ void __launch_bounds__(kStatsWarps * 32) level_stats_kernel(const uint4* __restrict__ levels,
+                                                                       const int* __restrict__ win_levels, int cap,
+                                                                       int N, int nwin, int n_src,
+                                                                       unsigned* __restrict__ stats, const int* gate) {
+  __shared__ unsigned s_part[kStatsWarps][kStatLevels][32];
+  if (gate && ld_volatile_i32(gate) == 0) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int v = blockIdx.x * 32 + lane;
+  unsigned acc[kStatLevels];
+#pragma unroll
+  for (int k = 0; k < kStatLevels; ++k) acc[k] = 0u;
+  if (v < N) {
+    for (int w = warp; w < nwin; w += kStatsWarps) {
+      const int base = w * 128;
+      const int l = min(128, n_src - base);
+      const int L = win_levels[w];
+      const int top = min(L > 0 ? L : cap, min(cap, kStatLevels - 1));
+      acc[0] += (unsigned)l - ((unsigned)(v - base) < (unsigned)l ? 1u : 0u);
+      const uint4* lev = levels + (size_t)w * (cap + 1) * N + v;
+#pragma unroll
+      for (int k = 1; k < kStatLevels; ++k)
+        if (k <= top) acc[k] += (unsigned)l - popc4(__ldg(lev + (size_t)k * N));
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < kStatLevels; ++k) s_part[warp][k][lane] = acc[k];
+  __syncthreads();
+  for (int i = threadIdx.x; i < 32 * kStatLevels; i += blockDim.x) {
+    const int vl = i / kStatLevels, k = i % kStatLevels;
+    const int vv = blockIdx.x * 32 + vl;
+    if (vv >= N) continue;
+    unsigned t = 0u;
+#pragma unroll
+    for (int q = 0; q < kStatsWarps; ++q) t += s_part[q][k][vl];
+    stats[(size_t)vv * kStatLevels + k] = t;
+  }
+}
+
 // ---- the delta evaluation: one CTA per (candidate, window), window-major ------------
 constexpr int kDeltaThreads = 256;
 constexpr int kDeltaRows = 512;        // dirty rows a task can hold per level
 constexpr int kDeltaHash = 1024;       // hash slots for the dirty rows (power of two)
 constexpr int kDeltaLevels = 48;       // levels a task may run past level 0
+constexpr int kGrp = 8;                // neighbour rows loaded together
 
 struct DeltaArgs {
   const uint4* levels;                 // base rows, R = 1: [nwin][level_cap + 1][N]
@@ -202,6 +250,46 @@ __global__ void __launch_bounds__(kDeltaThreads) delta_kernel(const DeltaArgs a)
     return __ldg(lev + (size_t)k * N + v);
   };
   // S'_k of row y: its dirty value when y is in D_k (table s_key), else the base
+  // slot of row y in D_k's table, or -1
+  auto dirty_slot = [&](int nd, int y) -> int {
+    if (nd > 0) {
+      unsigned h = ((unsigned)y * 2654435761u) & (kDeltaHash - 1);
+      for (int p = 0; p < kDeltaHash; ++p) {
+        const int key = s_key[h];
+        if (key == y) return s_slot[h];
+        if (key < 0) break;
+        h = (h + 1) & (kDeltaHash - 1);
+      }
+    }
+    return -1;
+  };
+  // S'_{k+1}[x] = S'_k[x] | OR_j S'_k[N'(x)_j]: neighbour ids, then their
+  // dirty slots (shared memory), then all row loads of a group at once
+  auto derive = [&](int k, int nd, int cur, int x) -> uint4 {
+    const int qx = x == X0 ? 0 : x == X1 ? 1 : x == X2 ? 2 : x == X3 ? 3 : -1;
+    const int px = qx >= 0 ? sw.pos[qx] : -1;
+    const int vx = qx >= 0 ? NV[qx] : 0;
+    const int* row = a.adj + (long long)x * d;
+    const int dx = dirty_slot(nd, x);
+    uint4 acc = dx >= 0 ? s_val[cur][dx] : base_row(k, x);
+    for (int j0 = 0; j0 < d; j0 += kGrp) {
+      int u[kGrp], ds[kGrp];
+#pragma unroll
+      for (int q = 0; q < kGrp; ++q) {
+        const int j = j0 + q;
+        u[q] = j < d ? (j == px ? vx : __ldg(row + j)) : -1;
+      }
+#pragma unroll
+      for (int q = 0; q < kGrp; ++q) ds[q] = u[q] >= 0 ? dirty_slot(nd, u[q]) : -1;
+      uint4 r[kGrp];
+#pragma unroll
+      for (int q = 0; q < kGrp; ++q)
+        r[q] = u[q] < 0 ? make_uint4(0u, 0u, 0u, 0u) : (ds[q] >= 0 ? s_val[cur][ds[q]] : base_row(k, u[q]));
+#pragma unroll
+      for (int q = 0; q < kGrp; ++q) or_into(acc, r[q]);
+    }
+    return acc;
+  };
   auto row_k = [&](int k, int nd, int cur, int y) -> uint4 {
     if (nd > 0) {
       unsigned h = ((unsigned)y * 2654435761u) & (kDeltaHash - 1);
@@ -236,8 +324,7 @@ __global__ void __launch_bounds__(kDeltaThreads) delta_kernel(const DeltaArgs a)
       }
       const unsigned bit = 1u << (x & 31);
       if (atomicOr(&s_claim[x >> 5], bit) & bit) continue;
-      uint4 acc = row_k(k, nd, cur, x);
-      for (int j = 0; j < d; ++j) or_into(acc, row_k(k, nd, cur, nb(x, j)));
+      const uint4 acc = derive(k, nd, cur, x);
       const uint4 bn = base_row(k + 1, x);
       if (!equal4(acc, bn)) {
         const int idx = atomicAdd(&s_n[nxt], 1);
@@ -312,7 +399,23 @@ __global__ void __launch_bounds__(kDeltaThreads) delta_kernel(const DeltaArgs a)
         unsigned long long cnt = 0;
         for (int v = threadIdx.x; v < N; v += blockDim.x) {
           uint4 acc = __ldcg(A + v);
-          for (int j = 0; j < d; ++j) or_into(acc, __ldcg(A + nb(v, j)));
+          const int qv = v == X0 ? 0 : v == X1 ? 1 : v == X2 ? 2 : v == X3 ? 3 : -1;
+          const int pv = qv >= 0 ? sw.pos[qv] : -1;
+          const int nvv = qv >= 0 ? NV[qv] : 0;
+          const int* row = a.adj + (long long)v * d;
+          for (int j0 = 0; j0 < d; j0 += kGrp) {
+            int u[kGrp];
+#pragma unroll
+            for (int q = 0; q < kGrp; ++q) {
+              const int j = j0 + q;
+              u[q] = j < d ? (j == pv ? nvv : __ldg(row + j)) : -1;
+            }
+            uint4 r[kGrp];
+#pragma unroll
+            for (int q = 0; q < kGrp; ++q) r[q] = u[q] >= 0 ? __ldcg(A + u[q]) : make_uint4(0u, 0u, 0u, 0u);
+#pragma unroll
+            for (int q = 0; q < kGrp; ++q) or_into(acc, r[q]);
+          }
           __stcg(B + v, acc);
           cnt += popc4(acc);
         }

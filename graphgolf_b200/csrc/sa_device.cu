@@ -688,12 +688,12 @@ int enqueue_profile(ggb_sa* a, const int* gate, cudaStream_t st) {
   return coop_launch(profile_kernel_for(a->pR), a->sms, profile_smem_for(a->pR), params, st);
 }
 
-// The base of the delta evaluation (and, with a filter, the statistics),
-// gated on *gate.
+// The base of the delta evaluation (and, with a filter, the per-vertex
+// statistics read back from its levels), gated on *gate.
 int enqueue_base(ggb_sa* a, const int* gate, cudaStream_t st) {
   SCUDA(cudaMemsetAsync(a->d_bctrl, 0, (size_t)(1 + a->base_teams) * sizeof(ggb::ApspCtrl), st));
   ggb::ApspArgs p = graph_args(a);
-  p.stats = a->learned ? a->d_stats : nullptr;
+  p.stats = nullptr;   // the filter's statistics are read back from the levels (level_stats_kernel)
   p.levels = a->d_levels;
   p.level_counts = a->d_lcounts;
   p.win_levels = a->d_winlev;
@@ -708,8 +708,14 @@ int enqueue_base(ggb_sa* a, const int* gate, cudaStream_t st) {
   b.n_teams = a->base_teams;
   b.team_ctas = a->base_T;
   void* params[] = {(void*)&p, (void*)&b};
-  return coop_launch((const void*)ggb::apsp_base_kernel<1>, a->base_teams * a->base_T, ggb::apsp_smem_bytes<1>(),
-                     params, st);
+  int rc = coop_launch((const void*)ggb::apsp_base_kernel<1>, a->base_teams * a->base_T, ggb::apsp_smem_bytes<1>(),
+                       params, st);
+  if (rc || !a->learned) return rc;
+  ggb::level_stats_kernel<<<(a->N + 31) / 32, ggb::kStatsWarps * 32, 0, st>>>(a->d_levels, a->d_winlev, a->level_cap, a->N, a->nwin,
+                                                             a->N, a->d_stats, gate);
+  ggb::core_add_launches(1);
+  SCUDA(cudaGetLastError());
+  return GGB_OK;
 }
 
 ggb::DeltaArgs delta_args(ggb_sa* a, const int* sel) {
@@ -923,11 +929,43 @@ int evaluate_current(ggb_sa* a) {
   return GGB_OK;
 }
 
+void set_base_team(ggb_sa* a, int T) {
+  a->base_T = T;
+  a->base_teams = std::max(1, std::min(a->sms / T, a->nwin));
+}
+
+// Times the base build of the current graph with teams of 1, 2, 4 and 8 CTAs
+// (two launches each after one warm-up) and keeps the fastest.  The result
+// never depends on the choice.
+int tune_base(ggb_sa* a) {
+  cudaEvent_t e0, e1;
+  SCUDA(cudaEventCreate(&e0));
+  SCUDA(cudaEventCreate(&e1));
+  float best = 1e30f;
+  int bestT = 4;
+  for (int T : {1, 2, 4, 8}) {
+    set_base_team(a, T);
+    int rc = enqueue_base(a, nullptr, a->st);
+    if (rc) return rc;
+    SCUDA(cudaEventRecord(e0, a->st));
+    for (int i = 0; i < 2 && !rc; ++i) rc = enqueue_base(a, nullptr, a->st);
+    if (rc) return rc;
+    SCUDA(cudaEventRecord(e1, a->st));
+    SCUDA(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    SCUDA(cudaEventElapsedTime(&ms, e0, e1));
+    if (ms < best) { best = ms; bestT = T; }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  set_base_team(a, bestT);
+  return check_sticky(a);
+}
+
 int alloc_base(ggb_sa* a) {
   a->nwin = (a->N + 127) / 128;
   a->level_cap = 15;
-  a->base_T = 4;
-  a->base_teams = std::max(1, std::min(a->sms / a->base_T, a->nwin));
+  set_base_team(a, 1);   // sizes the team arrays for the most teams any plan uses
   int nb = 0;
   SCUDA(cudaFuncSetAttribute((const void*)ggb::apsp_base_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)ggb::apsp_smem_bytes<1>()));
@@ -1050,10 +1088,8 @@ int create(ggb_sa* a, int nodes, int degree, const int* edges, int K, int G, int
   a->h.label_scale = 16.0f / (float)nodes;
   a->h.label_clip = 16.0f;
   if ((rc = push_state(a))) return rc;
+  if (a->delta && (rc = tune_base(a))) return rc;
   if ((rc = evaluate_current(a))) return rc;
-  if (a->learned && a->delta) {
-    // the statistics of the features come from the base build, which fills them
-  }
   if ((rc = push_state(a))) return rc;
   // batch slots hold the current graph until the first step
   for (ggb_batch* b : {a->cand, a->comp}) {
