@@ -133,7 +133,7 @@ CORE_SIGNATURES = {
     "ggb_sa_edges": (_I, [_P, _I, _P]),
     "ggb_sa_profile": (_I, [_P, _P]),
     "ggb_sa_last_step": (_I, [_P, _P, _P]),
-    "ggb_sa_check_delta": (_I, [_P, _IP, _IP, _IP]),
+    "ggb_sa_check_delta": (_I, [_P, _IP, _IP, _IP, _IP]),
 }
 
 HOST_SIGNATURES = {

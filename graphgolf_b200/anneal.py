@@ -106,12 +106,12 @@ class Annealer:
         _raise(self._lib.ggb_sa_last_step(self._h, pr.ctypes.data, lb.ctypes.data))
         return pr, lb
 
-    def check_delta(self) -> tuple[int, int, int]:
-        """(compared, mismatches, unevaluated): fresh candidates evaluated
-        against the base and in full."""
-        c, m, u = C.c_int(), C.c_int(), C.c_int()
-        _raise(self._lib.ggb_sa_check_delta(self._h, C.byref(c), C.byref(m), C.byref(u)))
-        return c.value, m.value, u.value
+    def check_delta(self, with_dense: bool = False):
+        """(compared, mismatches, unevaluated[, dense windows]): fresh
+        candidates evaluated against the base and in full."""
+        c, m, u, dn = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        _raise(self._lib.ggb_sa_check_delta(self._h, C.byref(c), C.byref(m), C.byref(u), C.byref(dn)))
+        return (c.value, m.value, u.value, dn.value) if with_dense else (c.value, m.value, u.value)
 
     def profile(self) -> np.ndarray:
         """[nodes][32]: entry [v][k] = vertices farther than k from v."""

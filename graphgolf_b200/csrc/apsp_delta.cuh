@@ -176,6 +176,11 @@ struct DeltaArgs {
   const int* stop;                     // nothing runs while *stop != 0 (may be null)
   long long* dsum;                     // [K][nwin] sum_k delta_k
   int* dlev;                           // [K][nwin] completion level; -1 stalled; -2 not evaluated
+  const unsigned* stats;               // base per-vertex statistics [N][kStatLevels]
+  long long* ep_sum;                   // [K][4] transmission of endpoint q in the candidate graph
+  int* ep_ecc;                         // [K][4] its eccentricity; -1 if some vertex is unreachable
+  unsigned short* ep_dist;             // [K][4][N] scratch of the endpoint searches: levels
+  int* ep_queue;                       // [K][4][N] and visit order
   uint4* dense_pool;                   // dense_slots slots of 2*N rows for tasks whose dirty set overflows
   int* dense_used;                     // slots taken (zeroed before the launch)
   int dense_slots;
@@ -212,7 +217,6 @@ __global__ void __launch_bounds__(kDeltaThreads) delta_kernel(const DeltaArgs a)
   const int N = a.N, d = a.d;
   const int base = w * 128;
   const int l = min(128, a.n_src - base);
-  const long long full_count = (long long)N * l;
   const int L = a.win_levels[w];
   long long* const out_sum = a.dsum + (size_t)c * a.nwin + w;
   int* const out_lev = a.dlev + (size_t)c * a.nwin + w;
@@ -223,7 +227,34 @@ __global__ void __launch_bounds__(kDeltaThreads) delta_kernel(const DeltaArgs a)
     }
     return;
   }
-  const uint4 fullm = chunk_full_mask(0, l);
+  // A swap endpoint's own distances change for many vertices; its source bit
+  // is masked out here and its distances come from endpoint_bfs_kernel.
+  // The masked window counts only the other sources: its base counts lose
+  // the endpoint's reached vertices, N - stats[x][k] at level k.
+  uint4 fullm = chunk_full_mask(0, l);
+  int nmask = 0, mv[4];
+  for (int q = 0; q < 4; ++q) {
+    const unsigned b = (unsigned)(sw.x[q] - base);
+    if (b < (unsigned)l) {
+      const unsigned m = ~(1u << (b & 31));
+      if ((b >> 5) == 0) fullm.x &= m; else if ((b >> 5) == 1) fullm.y &= m; else if ((b >> 5) == 2) fullm.z &= m; else fullm.w &= m;
+      mv[nmask++] = sw.x[q];
+    }
+  }
+  const int lm = l - nmask;
+  const long long full_count = (long long)N * lm;
+  auto masked_base_count = [&](int k, long long ck) -> long long {
+    for (int i = 0; i < nmask; ++i)
+      ck -= N - (long long)(k < kStatLevels ? __ldg(a.stats + (size_t)mv[i] * kStatLevels + k) : 0u);
+    return ck;
+  };
+  if (lm == 0) {                       // every source of the window is an endpoint
+    if (threadIdx.x == 0) {
+      *out_sum = 0;
+      *out_lev = 0;
+    }
+    return;
+  }
   const int cap = a.level_cap;
   const uint4* const lev = a.levels + (size_t)w * (cap + 1) * N;
   const long long* const lc = a.level_counts + (size_t)w * (cap + 1);
@@ -245,9 +276,10 @@ __global__ void __launch_bounds__(kDeltaThreads) delta_kernel(const DeltaArgs a)
     return __ldg(a.adj + (long long)x * d + j);
   };
   auto base_row = [&](int k, int v) -> uint4 {
-    if (k == 0) return identity_row(v, base, l);
     if (k > L) return fullm;
-    return __ldg(lev + (size_t)k * N + v);
+    uint4 r = k == 0 ? identity_row(v, base, l) : __ldg(lev + (size_t)k * N + v);
+    r.x &= fullm.x; r.y &= fullm.y; r.z &= fullm.z; r.w &= fullm.w;
+    return r;
   };
   // S'_k of row y: its dirty value when y is in D_k (table s_key), else the base
   // slot of row y in D_k's table, or -1
@@ -303,7 +335,7 @@ __global__ void __launch_bounds__(kDeltaThreads) delta_kernel(const DeltaArgs a)
     return base_row(k, y);
   };
   int cur = 0;
-  long long total_delta = 0, prev_count = l;
+  long long total_delta = 0, prev_count = lm;
   int Lc = -1;
   int status = -2;   // becomes the completion level, or -1 when the candidate stalls
   int k = 0;
@@ -370,7 +402,7 @@ __global__ void __launch_bounds__(kDeltaThreads) delta_kernel(const DeltaArgs a)
       s_slot[h] = i;
     }
     total_delta += delta;
-    const long long ck = (k + 1 <= L) ? lc[k + 1] : full_count;
+    const long long ck = (k + 1 <= L) ? masked_base_count(k + 1, lc[k + 1]) : full_count;
     const long long count = ck + delta;
     if (Lc < 0 && count == full_count) Lc = k + 1;
     __syncthreads();
@@ -425,7 +457,7 @@ __global__ void __launch_bounds__(kDeltaThreads) delta_kernel(const DeltaArgs a)
         __syncthreads();
         long long count = 0;
         for (int i = 0; i < kDeltaThreads / 32; ++i) count += (long long)s_red[i];
-        const long long ck = (k + 1 <= L) ? lc[k + 1] : full_count;
+        const long long ck = (k + 1 <= L) ? masked_base_count(k + 1, lc[k + 1]) : full_count;
         total_delta += count - ck;
         if (Lc < 0 && count == full_count) Lc = k + 1;
         if (Lc >= 0 && k + 1 >= L) { status = Lc; break; }
@@ -444,9 +476,67 @@ __global__ void __launch_bounds__(kDeltaThreads) delta_kernel(const DeltaArgs a)
   }
 }
 
-// Per candidate: the base's result changed by its windows' deltas, as the
-// record a batch evaluation writes (done = 0 when a window was not
-// evaluated).  One warp per candidate.
+// The distances from each endpoint x_q of candidate c in the candidate graph:
+// a level-synchronous breadth-first search, one CTA per (candidate,
+// endpoint), over a queue in scratch memory of this CTA's own (16-bit levels
+// and the visit order): a vertex is claimed by a 16-bit compare-and-swap, so
+// each level touches only its frontier's edges.  Gives the endpoint's
+// transmission and eccentricity (-1 when some vertex is unreachable).
+__global__ void __launch_bounds__(kDeltaThreads) endpoint_bfs_kernel(const DeltaArgs a) {
+  __shared__ int s_tail;
+  if (a.stop && ld_volatile_i32(a.stop) != 0) return;
+  const int c = blockIdx.x >> 2, q = blockIdx.x & 3;
+  const Swap sw = a.sw[a.sel ? a.sel[c] : c];
+  if (!sw.valid) return;
+  const int N = a.N, d = a.d;
+  const int X0 = sw.x[0], X1 = sw.x[1], X2 = sw.x[2], X3 = sw.x[3];
+  const int NV[4] = {X2, X3, X0, X1};
+  unsigned short* dist = a.ep_dist + ((size_t)c * 4 + q) * N;
+  int* queue = a.ep_queue + ((size_t)c * 4 + q) * N;
+  const int src = sw.x[q];
+  for (int v = threadIdx.x; v < N; v += blockDim.x) dist[v] = v == src ? 0 : 0xFFFF;
+  if (threadIdx.x == 0) {
+    queue[0] = src;
+    s_tail = 1;
+  }
+  __syncthreads();
+  long long tsum = 0;
+  int lo = 0, hi = 1, level = 0;
+  while (hi > lo) {
+    const unsigned short nxt = (unsigned short)(level + 1);
+    for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+      const int v = queue[i];
+      const int qv = v == X0 ? 0 : v == X1 ? 1 : v == X2 ? 2 : v == X3 ? 3 : -1;
+      const int pv = qv >= 0 ? sw.pos[qv] : -1;
+      const int* row = a.adj + (long long)v * d;
+      for (int j = 0; j < d; ++j) {
+        const int u = j == pv ? NV[qv] : __ldg(row + j);
+        if (dist[u] == 0xFFFF && atomicCAS(dist + u, (unsigned short)0xFFFF, nxt) == 0xFFFF)
+          queue[atomicAdd(&s_tail, 1)] = u;
+      }
+    }
+    __syncthreads();
+    lo = hi;
+    hi = s_tail;
+    if (hi > lo) {
+      tsum += (long long)(level + 1) * (hi - lo);
+      ++level;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    a.ep_sum[c * 4 + q] = tsum;
+    a.ep_ecc[c * 4 + q] = hi == N ? level : -1;
+  }
+}
+
+// Per candidate: the base's result changed by its windows' deltas and its
+// endpoints' searches, as the record a batch evaluation writes (done = 0
+// when a window was not evaluated).  With T the base transmission of an
+// endpoint (the sum of its statistics) and T' the searched one:
+//   sum' = sum - sum_{w,k} delta_{w,k} + sum_q (T'_q - T_q),
+//   diameter' = max(completion levels, endpoint eccentricities).
+// One warp per candidate.
 __global__ void delta_reduce_kernel(const DeltaArgs a, const BaseResult* __restrict__ base, BatchOut* __restrict__ out) {
   const int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
@@ -454,6 +544,15 @@ __global__ void delta_reduce_kernel(const DeltaArgs a, const BaseResult* __restr
   if (a.stop && ld_volatile_i32(a.stop) != 0) return;
   long long s = 0;
   int mx = 0, stalled = 0, missing = 0;
+  const Swap sw = a.sw[a.sel ? a.sel[c] : c];
+  if (sw.valid && lane < 4) {
+    const unsigned* st = a.stats + (size_t)sw.x[lane] * kStatLevels;
+    long long t = 0;
+    for (int k = 0; k < kStatLevels; ++k) t += st[k];
+    const int e = a.ep_ecc[c * 4 + lane];
+    s += t - a.ep_sum[c * 4 + lane];   // r.sum = base sum - s: adds T'_q - T_q
+    if (e < 0) stalled = 1; else mx = max(mx, e);
+  }
   for (int w = lane; w < a.nwin; w += 32) {
     s += a.dsum[(size_t)c * a.nwin + w];
     const int lv = a.dlev[(size_t)c * a.nwin + w];

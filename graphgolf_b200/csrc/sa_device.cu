@@ -605,6 +605,10 @@ struct ggb_sa {
   long long* d_dsum = nullptr;        // [K][nwin]
   int* d_dlev = nullptr;              // [K][nwin]
   ggb::BatchOut* d_dout = nullptr;    // [K]
+  long long* d_epsum = nullptr;       // [K][4] endpoint transmissions in the candidates
+  int* d_epecc = nullptr;             // [K][4]
+  unsigned short* d_epdist = nullptr; // [K][4][N] endpoint search scratch: levels
+  int* d_epqueue = nullptr;           // [K][4][N] and visit order
   uint4* d_dpool = nullptr;           // dense fallback slots of the delta evaluation
   int* d_dused = nullptr;
   int dense_slots = 0;
@@ -688,8 +692,9 @@ int enqueue_profile(ggb_sa* a, const int* gate, cudaStream_t st) {
   return coop_launch(profile_kernel_for(a->pR), a->sms, profile_smem_for(a->pR), params, st);
 }
 
-// The base of the delta evaluation (and, with a filter, the per-vertex
-// statistics read back from its levels), gated on *gate.
+// The base of the delta evaluation and the per-vertex statistics read back
+// from its levels (the delta path and the filter's features use them),
+// gated on *gate.
 int enqueue_base(ggb_sa* a, const int* gate, cudaStream_t st) {
   SCUDA(cudaMemsetAsync(a->d_bctrl, 0, (size_t)(1 + a->base_teams) * sizeof(ggb::ApspCtrl), st));
   ggb::ApspArgs p = graph_args(a);
@@ -710,7 +715,7 @@ int enqueue_base(ggb_sa* a, const int* gate, cudaStream_t st) {
   void* params[] = {(void*)&p, (void*)&b};
   int rc = coop_launch((const void*)ggb::apsp_base_kernel<1>, a->base_teams * a->base_T, ggb::apsp_smem_bytes<1>(),
                        params, st);
-  if (rc || !a->learned) return rc;
+  if (rc) return rc;
   ggb::level_stats_kernel<<<(a->N + 31) / 32, ggb::kStatsWarps * 32, 0, st>>>(a->d_levels, a->d_winlev, a->level_cap, a->N, a->nwin,
                                                              a->N, a->d_stats, gate);
   ggb::core_add_launches(1);
@@ -729,6 +734,11 @@ ggb::DeltaArgs delta_args(ggb_sa* a, const int* sel) {
   g.stop = &a->d_state->done;
   g.dsum = a->d_dsum;
   g.dlev = a->d_dlev;
+  g.stats = a->d_stats;
+  g.ep_sum = a->d_epsum;
+  g.ep_ecc = a->d_epecc;
+  g.ep_dist = a->d_epdist;
+  g.ep_queue = a->d_epqueue;
   g.dense_pool = a->d_dpool;
   g.dense_used = a->d_dused;
   g.dense_slots = a->dense_slots;
@@ -745,9 +755,10 @@ int enqueue_delta(ggb_sa* a, const int* sel, cudaStream_t st) {
   const ggb::DeltaArgs g = delta_args(a, sel);
   const size_t smem = (size_t)((a->N + 31) / 32) * sizeof(unsigned);
   SCUDA(cudaMemsetAsync(a->d_dused, 0, sizeof(int), st));
+  ggb::endpoint_bfs_kernel<<<a->K * 4, ggb::kDeltaThreads, 0, st>>>(g);
   ggb::delta_kernel<<<a->K * a->nwin, ggb::kDeltaThreads, smem, st>>>(g);
   ggb::delta_reduce_kernel<<<(a->K + 7) / 8, 256, 0, st>>>(g, a->d_bres, a->d_dout);
-  ggb::core_add_launches(2);
+  ggb::core_add_launches(3);
   SCUDA(cudaGetLastError());
   return GGB_OK;
 }
@@ -875,7 +886,8 @@ void destroy(ggb_sa* a) {
                   (void*)a->d_scores, (void*)a->d_rank, (void*)a->d_rank_key, (void*)a->d_X, (void*)a->d_stats,
                   (void*)a->d_sticky, (void*)a->d_pctrl, (void*)a->d_pbuf, (void*)a->d_levels, (void*)a->d_lcounts,
                   (void*)a->d_winlev, (void*)a->d_bctrl, (void*)a->d_bscratch, (void*)a->d_bres, (void*)a->d_dsum,
-                  (void*)a->d_dlev, (void*)a->d_dout, (void*)a->d_dpool, (void*)a->d_dused})
+                  (void*)a->d_dlev, (void*)a->d_dout, (void*)a->d_dpool, (void*)a->d_dused,
+                  (void*)a->d_epsum, (void*)a->d_epecc, (void*)a->d_epdist, (void*)a->d_epqueue})
     cudaFree(q);
   if (a->cand) ggb_batch_destroy(a->cand);
   if (a->comp) ggb_batch_destroy(a->comp);
@@ -982,7 +994,10 @@ int alloc_base(ggb_sa* a) {
     return rc;
   // dense fallback: up to 8 windows per candidate, at most 1 GiB
   a->dense_slots = (int)std::max<long long>(1, std::min<long long>(8LL * a->K, (1LL << 30) / (32LL * a->N)));
-  if ((rc = sdev(&a->d_dpool, (size_t)a->dense_slots * 2 * a->N)) || (rc = sdev(&a->d_dused, 1))) return rc;
+  if ((rc = sdev(&a->d_dpool, (size_t)a->dense_slots * 2 * a->N)) || (rc = sdev(&a->d_dused, 1)) ||
+      (rc = sdev(&a->d_epsum, (size_t)4 * a->K)) || (rc = sdev(&a->d_epecc, (size_t)4 * a->K)) ||
+      (rc = sdev(&a->d_epdist, (size_t)4 * a->K * a->N)) || (rc = sdev(&a->d_epqueue, (size_t)4 * a->K * a->N)))
+    return rc;
   return GGB_OK;
 }
 
@@ -1263,7 +1278,7 @@ int ggb_sa_last_step(ggb_sa* a, float* predicted, float* label) {
   return GGB_OK;
 }
 
-int ggb_sa_check_delta(ggb_sa* a, int* compared, int* mismatches, int* unevaluated) {
+int ggb_sa_check_delta(ggb_sa* a, int* compared, int* mismatches, int* unevaluated, int* dense_windows) {
   using namespace ggb::sa;
   if (!a || !compared || !mismatches || !unevaluated) return core_fail(GGB_EINVAL, "null pointer");
   if (!a->delta) return core_fail(GGB_EPERM, "the annealer does not use the delta evaluation");
@@ -1301,6 +1316,7 @@ int ggb_sa_check_delta(ggb_sa* a, int* compared, int* mismatches, int* unevaluat
   *compared = cmp;
   *mismatches = bad;
   *unevaluated = unev;
+  if (dense_windows) SCUDA(cudaMemcpy(dense_windows, a->d_dused, sizeof(int), cudaMemcpyDeviceToHost));
   return check_sticky(a);
 }
 

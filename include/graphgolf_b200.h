@@ -365,8 +365,9 @@ int ggb_sa_last_step(ggb_sa *a, float *predicted, float *label);
 /* Self-check of the delta evaluation (candidates > 1): draws `candidates`
  * fresh swaps of the current graph, evaluates them against the base and in
  * full, and counts the disagreements in diameter, connectivity or distance
- * sum among those the delta path served. */
-int ggb_sa_check_delta(ggb_sa *a, int *compared, int *mismatches, int *unevaluated);
+ * sum among those the delta path served; dense_windows (may be NULL)
+ * receives how many (candidate, window) tasks fell back to a dense sweep. */
+int ggb_sa_check_delta(ggb_sa *a, int *compared, int *mismatches, int *unevaluated, int *dense_windows);
 /* Per-vertex level statistics of the current graph, [nodes][32]: entry
  * [v][k] = vertices not within distance k of v. */
 int ggb_sa_profile(ggb_sa *a, unsigned *stats);
