@@ -479,12 +479,22 @@ int ggb_batch_upload(ggb_batch* b, const int* const* adj, void* stream) {
   cudaStream_t st = stream ? (cudaStream_t)stream : b->stream;
   // The staging buffer may still feed an earlier copy on this stream.
   BCUDA(cudaStreamSynchronize(st));
+  for (int i = 0; i < b->n; ++i)
+    if ((size_t)b->N[i] * b->d[i] && !adj[i]) return core_fail(GGB_EINVAL, "batch graph %d: null adjacency", i);
+  // Each graph's copy into the pinned buffer overlaps the DMA of the graphs
+  // before it (one DMA per ~512 KiB of staged graphs).
+  const long long flush = 128 * 1024;   // ints
+  long long pending = 0;                 // first int not yet sent
   for (int i = 0; i < b->n; ++i) {
     const size_t n = (size_t)b->N[i] * b->d[i];
-    if (n && !adj[i]) return core_fail(GGB_EINVAL, "batch graph %d: null adjacency", i);
     if (n) std::memcpy(b->h_adj + b->off[i], adj[i], n * sizeof(int));
+    const long long end = i + 1 < b->n ? b->off[i + 1] : b->adj_ints;
+    if (end - pending >= flush || i + 1 == b->n) {
+      BCUDA(cudaMemcpyAsync(b->d_adj + pending, b->h_adj + pending, (size_t)(end - pending) * sizeof(int),
+                            cudaMemcpyHostToDevice, st));
+      pending = end;
+    }
   }
-  BCUDA(cudaMemcpyAsync(b->d_adj, b->h_adj, (size_t)b->adj_ints * sizeof(int), cudaMemcpyHostToDevice, st));
   return GGB_OK;
 }
 

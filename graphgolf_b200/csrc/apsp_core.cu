@@ -460,8 +460,14 @@ int stage_adj(const int* adj, size_t n, cudaStream_t st) {
   if (n) {
     // The pinned copy must not be overwritten while a previous copy from it is
     // in flight: the stream is idle here (every host entry point waits).
-    std::memcpy(g.h_adj, adj, n * sizeof(int));
-    CUDA_TRY(cudaMemcpyAsync(g.d_adj, g.h_adj, n * sizeof(int), cudaMemcpyHostToDevice, st));
+    // Chunks of at most 512 KiB: the copy of chunk i into the pinned buffer
+    // overlaps the DMA of chunk i-1.
+    const size_t chunk = (size_t)128 * 1024;   // ints
+    for (size_t o = 0; o < n; o += chunk) {
+      const size_t m = std::min(chunk, n - o);
+      std::memcpy(g.h_adj + o, adj + o, m * sizeof(int));
+      CUDA_TRY(cudaMemcpyAsync(g.d_adj + o, g.h_adj + o, m * sizeof(int), cudaMemcpyHostToDevice, st));
+    }
   }
   return GGB_OK;
 }

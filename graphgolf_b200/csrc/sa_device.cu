@@ -1324,7 +1324,7 @@ int ggb_sa_profile(ggb_sa* a, unsigned* stats) {
   if (!a || !stats) return core_fail(GGB_EINVAL, "null pointer");
   SCUDA(cudaSetDevice(a->device));
   // the statistics the features read: from the base build when it makes them
-  int rc = (a->delta && a->learned) ? enqueue_base(a, nullptr, a->st) : enqueue_profile(a, nullptr, a->st);
+  int rc = a->delta ? enqueue_base(a, nullptr, a->st) : enqueue_profile(a, nullptr, a->st);
   if (rc) return rc;
   SCUDA(cudaStreamSynchronize(a->st));
   rc = check_sticky(a);
