@@ -67,6 +67,7 @@ class ggb_sa_stats(C.Structure):
         ("best_aspl", C.c_double),
         ("temp", C.c_double),
         ("done", C.c_int),
+        ("delta", C.c_int),
     ]
 
 

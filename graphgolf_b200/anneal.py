@@ -38,6 +38,7 @@ class Stats:
     best_aspl: float
     temp: float
     done: bool
+    delta: bool         # candidates evaluated against the kept base (else in full)
 
 
 class Annealer:
@@ -91,7 +92,8 @@ class Annealer:
         _raise(self._lib.ggb_sa_run(self._h, steps, C.byref(st)))
         return Stats(st.step, st.accepts, st.multi_accepts, st.moved_swaps, st.evals, st.pred_accepts,
                      st.unevaluated, st.cur_diam, st.best_diam,
-                     st.cur_total, st.best_total, st.cur_aspl, st.best_aspl, st.temp, bool(st.done))
+                     st.cur_total, st.best_total, st.cur_aspl, st.best_aspl, st.temp, bool(st.done),
+                     bool(st.delta))
 
     def edges(self, best: bool = False) -> np.ndarray:
         out = np.empty((self.lines, 2), dtype=np.int32)

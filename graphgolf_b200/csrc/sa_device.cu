@@ -570,6 +570,7 @@ struct ggb_sa {
   int C = 0, pred_max = 0;        // predicted composites (learned mode) and their largest size
   bool learned = false;
   bool delta = false;             // candidates evaluated against the base, not in full
+  bool has_base = false;          // the base is kept (delta evaluation, the filter's features)
   State h{};                      // host mirror of the device state
   State* d_state = nullptr;
   int* d_edges = nullptr;
@@ -824,7 +825,7 @@ int enqueue_step(ggb_sa* a, cudaStream_t st) {
     rc = ggb::mlp_train_rows(a->mlp, a->d_X, a->d_sel, a->d_labels, a->K, st);
     if (rc) return rc;
   }
-  if (a->delta) {
+  if (a->has_base) {
     rc = enqueue_base(a, &s->accepted, st);
     if (rc) return rc;
   } else if (a->learned) {
@@ -911,7 +912,7 @@ int check_sticky(ggb_sa* a) {
 int evaluate_current(ggb_sa* a) {
   long long sum = 0;
   int diam = 0, disc = 0;
-  if (a->delta) {
+  if (a->has_base) {
     int rc = enqueue_base(a, nullptr, a->st);
     if (rc) return rc;
     ggb::BaseResult r;
@@ -976,7 +977,7 @@ int tune_base(ggb_sa* a) {
 
 int alloc_base(ggb_sa* a) {
   a->nwin = (a->N + 127) / 128;
-  a->level_cap = 15;
+  // a->level_cap is set by create() from the initial graph's diameter
   set_base_team(a, 1);   // sizes the team arrays for the most teams any plan uses
   int nb = 0;
   SCUDA(cudaFuncSetAttribute((const void*)ggb::apsp_base_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1066,7 +1067,33 @@ int create(ggb_sa* a, int nodes, int degree, const int* edges, int K, int G, int
     if (nb < 1) return core_fail(GGB_ECUDA, "profile kernel R=%d cannot be resident", R);
   }
   if ((rc = sdev(&a->d_pbuf, (size_t)2 * nodes * a->pR))) return rc;
-  if (a->delta && (rc = alloc_base(a))) return rc;
+  if (a->delta) {
+    // The base keeps levels 0..diameter of every 128-source window: no
+    // window of a later current graph needs more, because no accepted move
+    // ever lengthens the diameter (general/sa.c:371-384).  When that does not
+    // fit in a quarter of the free device memory (or the initial graph is not
+    // connected, which create() reports below), candidates are evaluated in
+    // full instead.
+    rc = enqueue_profile(a, nullptr, a->st);
+    if (rc) return rc;
+    ggb::ApspCtrl c;
+    SCUDA(cudaMemcpyAsync(&c, a->d_pctrl, sizeof c, cudaMemcpyDeviceToHost, a->st));
+    SCUDA(cudaStreamSynchronize(a->st));
+    if ((rc = check_sticky(a))) return rc;
+    size_t free_b = 0, total_b = 0;
+    SCUDA(cudaMemGetInfo(&free_b, &total_b));
+    const double base_bytes = (double)((nodes + 127) / 128) * (c.diam + 1) * nodes * 16.0;
+    if (c.done && !c.disconnected && c.diam < nodes && base_bytes <= 0.25 * (double)free_b) {
+      a->level_cap = std::max(2, c.diam);
+      if ((rc = alloc_base(a))) return rc;
+      a->has_base = true;
+    } else {
+      a->delta = false;
+      if (a->learned)
+        return core_fail(GGB_EINVAL, "the proposal filter reads its features from the base, which does not fit "
+                                     "(%.1f GB for this graph)", base_bytes / 1e9);
+    }
+  }
   // the candidate batch (full mode) and the composite batch
   const int nc = 1 + a->C;
   const int nmax = std::max(K, nc);
@@ -1103,9 +1130,33 @@ int create(ggb_sa* a, int nodes, int degree, const int* edges, int K, int G, int
   a->h.label_scale = 16.0f / (float)nodes;
   a->h.label_clip = 16.0f;
   if ((rc = push_state(a))) return rc;
-  if (a->delta && (rc = tune_base(a))) return rc;
+  if (a->has_base && (rc = tune_base(a))) return rc;
   if ((rc = evaluate_current(a))) return rc;
   if ((rc = push_state(a))) return rc;
+  if (a->delta) {
+    // One trial step of the delta path: when more than a quarter of the
+    // candidates cannot be served (graphs whose swaps change most distances,
+    // e.g. sparse graphs of large diameter), candidates are evaluated in full.
+    gen_kernel<<<(K + 127) / 128, 128, 0, a->st>>>(a->d_state, a->d_swaps, K);
+    if ((rc = enqueue_delta(a, nullptr, a->st))) return rc;
+    std::vector<ggb::BatchOut> t(K);
+    SCUDA(cudaMemcpyAsync(t.data(), a->d_dout, K * sizeof(ggb::BatchOut), cudaMemcpyDeviceToHost, a->st));
+    SCUDA(cudaStreamSynchronize(a->st));
+    if ((rc = check_sticky(a))) return rc;
+    int unserved = 0;
+    for (const auto& o : t) unserved += o.done ? 0 : 1;
+    if (4 * unserved > K) {
+      a->delta = false;
+      if ((rc = ggb_batch_create(K, nn.data(), bn.data(), gg.data(), dd.data(), &a->cand))) return rc;
+      a->cand->stop = &a->d_state->done;
+      a->cand->sticky = a->d_sticky;
+      for (int k = 0; k < K; ++k) {
+        int* slot = nullptr;
+        ggb_batch_adj_device(a->cand, k, &slot);
+        SCUDA(cudaMemcpy(slot, a->d_adj, adj.size() * sizeof(int), cudaMemcpyDeviceToDevice));
+      }
+    }
+  }
   // batch slots hold the current graph until the first step
   for (ggb_batch* b : {a->cand, a->comp}) {
     if (!b) continue;
@@ -1242,6 +1293,7 @@ int ggb_sa_run(ggb_sa* a, long long steps, ggb_sa_stats* stats) {
     stats->moved_swaps = a->h.moved_swaps;
     stats->pred_accepts = a->h.pred_accepts;
     stats->unevaluated = a->h.unevaluated;
+    stats->delta = a->delta ? 1 : 0;
     stats->evals = a->h.evals;
     stats->cur_diam = a->h.cur_diam;
     stats->best_diam = a->h.best_diam;
@@ -1281,7 +1333,7 @@ int ggb_sa_last_step(ggb_sa* a, float* predicted, float* label) {
 int ggb_sa_check_delta(ggb_sa* a, int* compared, int* mismatches, int* unevaluated, int* dense_windows) {
   using namespace ggb::sa;
   if (!a || !compared || !mismatches || !unevaluated) return core_fail(GGB_EINVAL, "null pointer");
-  if (!a->delta) return core_fail(GGB_EPERM, "the annealer does not use the delta evaluation");
+  if (!a->has_base) return core_fail(GGB_EPERM, "the annealer keeps no base for the delta evaluation");
   SCUDA(cudaSetDevice(a->device));
   int rc = pull_state(a);
   if (rc) return rc;
@@ -1324,7 +1376,7 @@ int ggb_sa_profile(ggb_sa* a, unsigned* stats) {
   if (!a || !stats) return core_fail(GGB_EINVAL, "null pointer");
   SCUDA(cudaSetDevice(a->device));
   // the statistics the features read: from the base build when it makes them
-  int rc = a->delta ? enqueue_base(a, nullptr, a->st) : enqueue_profile(a, nullptr, a->st);
+  int rc = a->has_base ? enqueue_base(a, nullptr, a->st) : enqueue_profile(a, nullptr, a->st);
   if (rc) return rc;
   SCUDA(cudaStreamSynchronize(a->st));
   rc = check_sticky(a);

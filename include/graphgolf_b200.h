@@ -335,6 +335,9 @@ typedef struct ggb_sa_stats {
   double cur_aspl, best_aspl;
   double temp;
   int done;                          /* the target was reached */
+  int delta;                         /* 1: candidates evaluated against the kept base (exact);
+                                        0: in full (plain mode, or graphs where the delta path
+                                        would not serve most candidates) */
 } ggb_sa_stats;
 
 /* edges: [nodes*degree/2][2] (a simple degree-regular graph, connected).

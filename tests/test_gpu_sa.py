@@ -47,13 +47,32 @@ def test_delta_evaluation_exact(gpu, n, d, K):
     before and after the base is rebuilt by accepted moves."""
     g = graphs.random_regular(n, d, n + d)
     with gg.Annealer(g, candidates=K, compose=8, seed=6) as an:
-        total = 0
         for rounds in range(3):
             c, m, u = an.check_delta()
             assert m == 0 and c + u == K and c >= K // 2
-            total += c
             an.run(3)
-        _check(an, g, an.run(0))
+        st = an.run(0)
+        assert st.delta
+        _check(an, g, st)
+
+
+def test_large_diameter_graph(gpu):
+    """A random 3-regular graph of 20000 vertices (diameter above 15): the
+    base keeps as many levels as the initial diameter, whatever the delta
+    path serves agrees with the full evaluation, and the annealer (on the
+    delta path or, where it would not serve, in full) accepts moves with
+    exact states."""
+    g = graphs.random_regular(20000, 3, 5)
+    assert gg.evaluate(g.adj).diameter > 15
+    with gg.Annealer(g, candidates=32, compose=8, seed=2) as an:
+        c, m, u = an.check_delta()
+        assert m == 0 and c + u == 32
+        st = an.run(5)
+        # a swap of a sparse graph of large diameter changes most distances: the
+        # annealer measured that at creation and evaluates its candidates in full
+        assert st.delta == (u * 4 <= 32)
+        assert st.accepts > 0
+        _check(an, g, st)
 
 
 def test_metropolis_states_exact(gpu):
