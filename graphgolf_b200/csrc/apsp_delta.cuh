@@ -202,7 +202,8 @@ __device__ __forceinline__ uint4 identity_row(int v, int base, int l) {
 }
 
 __global__ void __launch_bounds__(kDeltaThreads) delta_kernel(const DeltaArgs a) {
-  extern __shared__ unsigned s_claim[];                 // [ceil(N/32)]: rows claimed this level
+  extern __shared__ unsigned s_claim[];                 // [ceil(N/32)]: rows claimed this level, then
+                                                        // [ceil(N/32)]: rows in D_k (s_dbits)
   __shared__ int s_ids[2][kDeltaRows];
   __shared__ uint4 s_val[2][kDeltaRows];
   __shared__ int s_key[kDeltaHash];
@@ -259,7 +260,8 @@ __global__ void __launch_bounds__(kDeltaThreads) delta_kernel(const DeltaArgs a)
   const uint4* const lev = a.levels + (size_t)w * (cap + 1) * N;
   const long long* const lc = a.level_counts + (size_t)w * (cap + 1);
   const int nclaim = (N + 31) / 32;
-  for (int i = threadIdx.x; i < nclaim; i += blockDim.x) s_claim[i] = 0u;
+  unsigned* const s_dbits = s_claim + nclaim;
+  for (int i = threadIdx.x; i < 2 * nclaim; i += blockDim.x) s_claim[i] = 0u;
   for (int i = threadIdx.x; i < kDeltaHash; i += blockDim.x) s_key[i] = -1;
   if (threadIdx.x == 0) {
     s_n[0] = 0;
@@ -282,9 +284,9 @@ __global__ void __launch_bounds__(kDeltaThreads) delta_kernel(const DeltaArgs a)
     return r;
   };
   // S'_k of row y: its dirty value when y is in D_k (table s_key), else the base
-  // slot of row y in D_k's table, or -1
+  // slot of row y in D_k's table, or -1 (the bitmap answers most lookups)
   auto dirty_slot = [&](int nd, int y) -> int {
-    if (nd > 0) {
+    if (nd > 0 && ((s_dbits[y >> 5] >> (y & 31)) & 1u)) {
       unsigned h = ((unsigned)y * 2654435761u) & (kDeltaHash - 1);
       for (int p = 0; p < kDeltaHash; ++p) {
         const int key = s_key[h];
@@ -323,7 +325,7 @@ __global__ void __launch_bounds__(kDeltaThreads) delta_kernel(const DeltaArgs a)
     return acc;
   };
   auto row_k = [&](int k, int nd, int cur, int y) -> uint4 {
-    if (nd > 0) {
+    if (nd > 0 && ((s_dbits[y >> 5] >> (y & 31)) & 1u)) {
       unsigned h = ((unsigned)y * 2654435761u) & (kDeltaHash - 1);
       for (int p = 0; p < kDeltaHash; ++p) {
         const int key = s_key[h];
@@ -391,8 +393,10 @@ __global__ void __launch_bounds__(kDeltaThreads) delta_kernel(const DeltaArgs a)
     if (s_over) { dense = true; break; }   // D_k and its table are still intact
     long long delta = 0;
     for (int i = 0; i < kDeltaThreads / 32; ++i) delta += (long long)s_red[i];
-    // the next level's lookup table
+    // the next level's lookup table and bitmap (every set bit is a D_k row,
+    // so clearing the words of D_k's rows clears the bitmap)
     for (int i = threadIdx.x; i < kDeltaHash; i += blockDim.x) s_key[i] = -1;
+    for (int i = threadIdx.x; i < nd; i += blockDim.x) s_dbits[s_ids[cur][i] >> 5] = 0u;
     __syncthreads();
     const int nn = s_n[nxt];
     for (int i = threadIdx.x; i < nn; i += blockDim.x) {
@@ -400,6 +404,7 @@ __global__ void __launch_bounds__(kDeltaThreads) delta_kernel(const DeltaArgs a)
       unsigned h = ((unsigned)y * 2654435761u) & (kDeltaHash - 1);
       while (atomicCAS(&s_key[h], -1, y) != -1) h = (h + 1) & (kDeltaHash - 1);
       s_slot[h] = i;
+      atomicOr(&s_dbits[y >> 5], 1u << (y & 31));
     }
     total_delta += delta;
     const long long ck = (k + 1 <= L) ? masked_base_count(k + 1, lc[k + 1]) : full_count;

@@ -754,7 +754,7 @@ ggb::DeltaArgs delta_args(ggb_sa* a, const int* sel) {
 
 int enqueue_delta(ggb_sa* a, const int* sel, cudaStream_t st) {
   const ggb::DeltaArgs g = delta_args(a, sel);
-  const size_t smem = (size_t)((a->N + 31) / 32) * sizeof(unsigned);
+  const size_t smem = 2 * (size_t)((a->N + 31) / 32) * sizeof(unsigned);   // claims, dirty bitmap
   SCUDA(cudaMemsetAsync(a->d_dused, 0, sizeof(int), st));
   ggb::endpoint_bfs_kernel<<<a->K * 4, ggb::kDeltaThreads, 0, st>>>(g);
   ggb::delta_kernel<<<a->K * a->nwin, ggb::kDeltaThreads, smem, st>>>(g);
