@@ -179,8 +179,6 @@ struct DeltaArgs {
   const unsigned* stats;               // base per-vertex statistics [N][kStatLevels]
   long long* ep_sum;                   // [K][4] transmission of endpoint q in the candidate graph
   int* ep_ecc;                         // [K][4] its eccentricity; -1 if some vertex is unreachable
-  unsigned short* ep_dist;             // [K][4][N] scratch of the endpoint searches: levels
-  int* ep_queue;                       // [K][4][N] and visit order
   uint4* dense_pool;                   // dense_slots slots of 2*N rows for tasks whose dirty set overflows
   int* dense_used;                     // slots taken (zeroed before the launch)
   int dense_slots;
@@ -229,7 +227,7 @@ __global__ void __launch_bounds__(kDeltaThreads) delta_kernel(const DeltaArgs a)
     return;
   }
   // A swap endpoint's own distances change for many vertices; its source bit
-  // is masked out here and its distances come from endpoint_bfs_kernel.
+  // is masked out here and its distances come from endpoint_sweep_kernel.
   // The masked window counts only the other sources: its base counts lose
   // the endpoint's reached vertices, N - stats[x][k] at level k.
   uint4 fullm = chunk_full_mask(0, l);
@@ -481,57 +479,139 @@ __global__ void __launch_bounds__(kDeltaThreads) delta_kernel(const DeltaArgs a)
   }
 }
 
-// The distances from each endpoint x_q of candidate c in the candidate graph:
-// a level-synchronous breadth-first search, one CTA per (candidate,
-// endpoint), over a queue in scratch memory of this CTA's own (16-bit levels
-// and the visit order): a vertex is claimed by a 16-bit compare-and-swap, so
-// each level touches only its frontier's edges.  Gives the endpoint's
-// transmission and eccentricity (-1 when some vertex is unreachable).
-__global__ void __launch_bounds__(kDeltaThreads) endpoint_bfs_kernel(const DeltaArgs a) {
-  __shared__ int s_tail;
-  if (a.stop && ld_volatile_i32(a.stop) != 0) return;
-  const int c = blockIdx.x >> 2, q = blockIdx.x & 3;
-  const Swap sw = a.sw[a.sel ? a.sel[c] : c];
-  if (!sw.valid) return;
-  const int N = a.N, d = a.d;
-  const int X0 = sw.x[0], X1 = sw.x[1], X2 = sw.x[2], X3 = sw.x[3];
-  const int NV[4] = {X2, X3, X0, X1};
-  unsigned short* dist = a.ep_dist + ((size_t)c * 4 + q) * N;
-  int* queue = a.ep_queue + ((size_t)c * 4 + q) * N;
-  const int src = sw.x[q];
-  for (int v = threadIdx.x; v < N; v += blockDim.x) dist[v] = v == src ? 0 : 0xFFFF;
-  if (threadIdx.x == 0) {
-    queue[0] = src;
-    s_tail = 1;
+// ---- the endpoints' own distances: one bit-parallel search ------------------------
+// The distances from every endpoint x_q of every candidate c, each in its
+// own candidate graph, as one bit-parallel breadth-first search: source bit
+// i = 4c + q (one 32-bit word per lane, nw <= 32 words per vertex row), the
+// recurrence S_{k+1}[v] = S_k[v] | OR_{u in N(v)} S_k[u] of the evaluator
+// over the base adjacency, and then, for every row x_q(c) a candidate
+// patched, candidate c's four bits re-derived with its swapped neighbour
+// list (only those rows differ in c's graph).  Per source bit the sum of the
+// levels at which vertices are first reached is its transmission, the last
+// level that reaches a vertex its eccentricity.  Cooperative launch, one
+// 512-thread CTA per SM, levels separated by the bounded grid barrier.
+struct EndpointArgs {
+  const int* adj;                      // base adjacency [N][d], d <= 32
+  const Swap* sw;
+  const int* sel;
+  const int* stop;
+  ApspCtrl* ctrl;                      // grid barrier, zeroed before the launch
+  unsigned* rows;                      // 2 * N * nw words
+  int* head;                           // [N] first fix-up of a row (-1: none)
+  int* next;                           // [4K] next fix-up of the same row
+  unsigned* changed;                   // [kDeltaLevels]: any bit set at that level
+  unsigned* newbits;                   // [kDeltaLevels][nw]: sources that reached a vertex at that level
+  unsigned* tsum;                      // [nw * 32] per source: sum of distances
+  unsigned* unreach;                   // [nw] sources with an unreachable vertex
+  long long* ep_sum;                   // [K][4] outputs
+  int* ep_ecc;                         // [K][4]: -1 unreachable vertex, -2 did not converge
+  long long timeout_ns;
+  int N, d, K, nw;
+};
+
+__global__ void __launch_bounds__(kThreads, 1) endpoint_sweep_kernel(const EndpointArgs e) {
+  __shared__ int s_flag;
+  __shared__ unsigned s_t[32 * 32];
+  if (e.stop && ld_volatile_i32(e.stop) != 0) return;   // written before the launch: the same in every CTA
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long nthreads = (long long)gridDim.x * blockDim.x;
+  const int gw = blockIdx.x * kWarps + warp, nwarps = gridDim.x * kWarps;
+  const int N = e.N, d = e.d, nw = e.nw, nsrc = 4 * e.K;
+  unsigned* A = e.rows;
+  unsigned* B = e.rows + (size_t)N * nw;
+  // phase 0: clear
+  for (long long i = tid; i < (long long)N * nw; i += nthreads) A[i] = 0u;
+  for (long long i = tid; i < N; i += nthreads) e.head[i] = -1;
+  for (long long i = tid; i < (long long)kDeltaLevels * nw; i += nthreads) e.newbits[i] = 0u;
+  for (long long i = tid; i < kDeltaLevels; i += nthreads) e.changed[i] = 0u;
+  for (long long i = tid; i < 32 * nw; i += nthreads) e.tsum[i] = 0u;
+  for (long long i = tid; i < nw; i += nthreads) e.unreach[i] = 0u;
+  for (int i = threadIdx.x; i < 32 * 32; i += blockDim.x) s_t[i] = 0u;
+  unsigned long long bar = gridDim.x;
+  if (!grid_barrier(e.ctrl, bar, e.timeout_ns, &s_flag)) return;
+  // phase 1: identity bits and the fix-up lists of the patched rows
+  for (long long i = tid; i < nsrc; i += nthreads) {
+    const int c = (int)i >> 2, q = (int)i & 3;
+    const Swap w = e.sw[e.sel ? e.sel[c] : c];
+    if (!w.valid) continue;
+    const int v = w.x[q];
+    atomicOr(A + (size_t)v * nw + (i >> 5), 1u << (i & 31));
+    e.next[i] = atomicExch(e.head + v, (int)i);
   }
-  __syncthreads();
-  long long tsum = 0;
-  int lo = 0, hi = 1, level = 0;
-  while (hi > lo) {
-    const unsigned short nxt = (unsigned short)(level + 1);
-    for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) {
-      const int v = queue[i];
-      const int qv = v == X0 ? 0 : v == X1 ? 1 : v == X2 ? 2 : v == X3 ? 3 : -1;
-      const int pv = qv >= 0 ? sw.pos[qv] : -1;
-      const int* row = a.adj + (long long)v * d;
+  bar += gridDim.x;
+  if (!grid_barrier(e.ctrl, bar, e.timeout_ns, &s_flag)) return;
+  unsigned T[32];
+#pragma unroll
+  for (int b = 0; b < 32; ++b) T[b] = 0u;
+  int L = 0;
+  bool converged = false;
+  for (; L < kDeltaLevels; ++L) {
+    unsigned ornew = 0u;
+    for (int v = gw; v < N; v += nwarps) {
+      const int nb = lane < d ? __ldg(e.adj + (long long)v * d + lane) : 0;
+      const unsigned own = lane < nw ? __ldcg(A + (size_t)v * nw + lane) : 0u;
+      unsigned acc = own;
       for (int j = 0; j < d; ++j) {
-        const int u = j == pv ? NV[qv] : __ldg(row + j);
-        if (dist[u] == 0xFFFF && atomicCAS(dist + u, (unsigned short)0xFFFF, nxt) == 0xFFFF)
-          queue[atomicAdd(&s_tail, 1)] = u;
+        const int u = __shfl_sync(0xffffffffu, nb, j);
+        if (lane < nw) acc |= __ldcg(A + (size_t)u * nw + lane);
+      }
+      for (int f = __ldcg(e.head + v); f >= 0; f = __ldcg(e.next + f)) {   // the same list in every lane
+        const int c = f >> 2, q = f & 3;
+        const Swap w = e.sw[e.sel ? e.sel[c] : c];
+        const int wc = (4 * c) >> 5;
+        const unsigned m = 0xFu << ((4 * c) & 31);
+        const int nv = q == 0 ? w.x[2] : q == 1 ? w.x[3] : q == 2 ? w.x[0] : w.x[1];
+        unsigned accc = own;
+        for (int j = 0; j < d; ++j) {
+          int u = __shfl_sync(0xffffffffu, nb, j);
+          if (j == w.pos[q]) u = nv;
+          if (lane == wc) accc |= __ldcg(A + (size_t)u * nw + wc);
+        }
+        if (lane == wc) acc = (acc & ~m) | (accc & m);
+      }
+      if (lane < nw) {
+        const unsigned nb_new = acc & ~own;
+        __stcg(B + (size_t)v * nw + lane, acc);
+        ornew |= nb_new;
+#pragma unroll
+        for (int b = 0; b < 32; ++b) T[b] += ((nb_new >> b) & 1u) ? (unsigned)(L + 1) : 0u;
       }
     }
-    __syncthreads();
-    lo = hi;
-    hi = s_tail;
-    if (hi > lo) {
-      tsum += (long long)(level + 1) * (hi - lo);
-      ++level;
+    if (lane < nw && ornew) {
+      atomicOr(e.newbits + (size_t)L * nw + lane, ornew);
+      atomicOr(e.changed + L, 1u);
     }
-    __syncthreads();
+    bar += gridDim.x;
+    if (!grid_barrier(e.ctrl, bar, e.timeout_ns, &s_flag)) return;
+    if (ld_volatile_i32(reinterpret_cast<const int*>(e.changed + L)) == 0) { converged = true; break; }
+    unsigned* t = A;
+    A = B;
+    B = t;
   }
-  if (threadIdx.x == 0) {
-    a.ep_sum[c * 4 + q] = tsum;
-    a.ep_ecc[c * 4 + q] = hi == N ? level : -1;
+  // A holds the final rows: sources with a vertex never reached, and the sums
+  if (lane < nw) {
+    unsigned un = 0u;
+    for (int v = gw; v < N; v += nwarps) un |= ~__ldcg(A + (size_t)v * nw + lane);
+    if (un) atomicOr(e.unreach + lane, un);
+#pragma unroll
+    for (int b = 0; b < 32; ++b)
+      if (T[b]) atomicAdd(s_t + lane * 32 + b, T[b]);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < 32 * nw; i += blockDim.x)
+    if (s_t[i]) atomicAdd(e.tsum + i, s_t[i]);
+  bar += gridDim.x;
+  if (!grid_barrier(e.ctrl, bar, e.timeout_ns, &s_flag)) return;
+  if (blockIdx.x == 0) {
+    for (int i = threadIdx.x; i < nsrc; i += blockDim.x) {
+      int ecc = 0;
+      for (int k = 0; k < L; ++k)
+        if ((__ldcg(e.newbits + (size_t)k * nw + (i >> 5)) >> (i & 31)) & 1u) ecc = k + 1;
+      const bool un = (__ldcg(e.unreach + (i >> 5)) >> (i & 31)) & 1u;
+      e.ep_sum[i] = (long long)__ldcg(e.tsum + i);
+      e.ep_ecc[i] = !converged ? -2 : (un ? -1 : ecc);
+    }
   }
 }
 
@@ -556,7 +636,9 @@ __global__ void delta_reduce_kernel(const DeltaArgs a, const BaseResult* __restr
     for (int k = 0; k < kStatLevels; ++k) t += st[k];
     const int e = a.ep_ecc[c * 4 + lane];
     s += t - a.ep_sum[c * 4 + lane];   // r.sum = base sum - s: adds T'_q - T_q
-    if (e < 0) stalled = 1; else mx = max(mx, e);
+    if (e == -1) stalled = 1;
+    else if (e < 0) missing = 1;
+    else mx = max(mx, e);
   }
   for (int w = lane; w < a.nwin; w += 32) {
     s += a.dsum[(size_t)c * a.nwin + w];

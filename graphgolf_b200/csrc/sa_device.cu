@@ -608,8 +608,13 @@ struct ggb_sa {
   ggb::BatchOut* d_dout = nullptr;    // [K]
   long long* d_epsum = nullptr;       // [K][4] endpoint transmissions in the candidates
   int* d_epecc = nullptr;             // [K][4]
-  unsigned short* d_epdist = nullptr; // [K][4][N] endpoint search scratch: levels
-  int* d_epqueue = nullptr;           // [K][4][N] and visit order
+  // the endpoints' bit-parallel search
+  int ep_nw = 0;                      // words per row: ceil(4K / 32)
+  unsigned* d_eprows = nullptr;       // [2][N][ep_nw]
+  int* d_ephead = nullptr;            // [N]
+  int* d_epnext = nullptr;            // [4K]
+  unsigned* d_epmisc = nullptr;       // changed [kDeltaLevels], newbits [kDeltaLevels][32], tsum [1024], unreach [32]
+  ggb::ApspCtrl* d_epctrl = nullptr;
   uint4* d_dpool = nullptr;           // dense fallback slots of the delta evaluation
   int* d_dused = nullptr;
   int dense_slots = 0;
@@ -738,8 +743,6 @@ ggb::DeltaArgs delta_args(ggb_sa* a, const int* sel) {
   g.stats = a->d_stats;
   g.ep_sum = a->d_epsum;
   g.ep_ecc = a->d_epecc;
-  g.ep_dist = a->d_epdist;
-  g.ep_queue = a->d_epqueue;
   g.dense_pool = a->d_dpool;
   g.dense_used = a->d_dused;
   g.dense_slots = a->dense_slots;
@@ -756,7 +759,32 @@ int enqueue_delta(ggb_sa* a, const int* sel, cudaStream_t st) {
   const ggb::DeltaArgs g = delta_args(a, sel);
   const size_t smem = 2 * (size_t)((a->N + 31) / 32) * sizeof(unsigned);   // claims, dirty bitmap
   SCUDA(cudaMemsetAsync(a->d_dused, 0, sizeof(int), st));
-  ggb::endpoint_bfs_kernel<<<a->K * 4, ggb::kDeltaThreads, 0, st>>>(g);
+  {
+    ggb::EndpointArgs e;
+    e.adj = a->d_adj;
+    e.sw = a->d_swaps;
+    e.sel = sel;
+    e.stop = &a->d_state->done;
+    e.ctrl = a->d_epctrl;
+    e.rows = a->d_eprows;
+    e.head = a->d_ephead;
+    e.next = a->d_epnext;
+    e.changed = a->d_epmisc;
+    e.newbits = a->d_epmisc + ggb::kDeltaLevels;
+    e.tsum = e.newbits + ggb::kDeltaLevels * 32;
+    e.unreach = e.tsum + 1024;
+    e.ep_sum = a->d_epsum;
+    e.ep_ecc = a->d_epecc;
+    e.timeout_ns = 2000000000LL;
+    e.N = a->N;
+    e.d = a->d;
+    e.K = a->K;
+    e.nw = a->ep_nw;
+    SCUDA(cudaMemsetAsync(a->d_epctrl, 0, sizeof(ggb::ApspCtrl), st));
+    void* params[] = {(void*)&e};
+    int rc = coop_launch((const void*)ggb::endpoint_sweep_kernel, a->sms, 0, params, st);
+    if (rc) return rc;
+  }
   ggb::delta_kernel<<<a->K * a->nwin, ggb::kDeltaThreads, smem, st>>>(g);
   ggb::delta_reduce_kernel<<<(a->K + 7) / 8, 256, 0, st>>>(g, a->d_bres, a->d_dout);
   ggb::core_add_launches(3);
@@ -888,7 +916,8 @@ void destroy(ggb_sa* a) {
                   (void*)a->d_sticky, (void*)a->d_pctrl, (void*)a->d_pbuf, (void*)a->d_levels, (void*)a->d_lcounts,
                   (void*)a->d_winlev, (void*)a->d_bctrl, (void*)a->d_bscratch, (void*)a->d_bres, (void*)a->d_dsum,
                   (void*)a->d_dlev, (void*)a->d_dout, (void*)a->d_dpool, (void*)a->d_dused,
-                  (void*)a->d_epsum, (void*)a->d_epecc, (void*)a->d_epdist, (void*)a->d_epqueue})
+                  (void*)a->d_epsum, (void*)a->d_epecc, (void*)a->d_eprows, (void*)a->d_ephead,
+                  (void*)a->d_epnext, (void*)a->d_epmisc, (void*)a->d_epctrl})
     cudaFree(q);
   if (a->cand) ggb_batch_destroy(a->cand);
   if (a->comp) ggb_batch_destroy(a->comp);
@@ -997,8 +1026,11 @@ int alloc_base(ggb_sa* a) {
   a->dense_slots = (int)std::max<long long>(1, std::min<long long>(8LL * a->K, (1LL << 30) / (32LL * a->N)));
   if ((rc = sdev(&a->d_dpool, (size_t)a->dense_slots * 2 * a->N)) || (rc = sdev(&a->d_dused, 1)) ||
       (rc = sdev(&a->d_epsum, (size_t)4 * a->K)) || (rc = sdev(&a->d_epecc, (size_t)4 * a->K)) ||
-      (rc = sdev(&a->d_epdist, (size_t)4 * a->K * a->N)) || (rc = sdev(&a->d_epqueue, (size_t)4 * a->K * a->N)))
+      (rc = sdev(&a->d_eprows, (size_t)2 * a->N * ((4 * a->K + 31) / 32))) || (rc = sdev(&a->d_ephead, (size_t)a->N)) ||
+      (rc = sdev(&a->d_epnext, (size_t)4 * a->K)) ||
+      (rc = sdev(&a->d_epmisc, (size_t)ggb::kDeltaLevels * 33 + 1024 + 32)) || (rc = sdev(&a->d_epctrl, 1)))
     return rc;
+  a->ep_nw = (4 * a->K + 31) / 32;
   return GGB_OK;
 }
 
@@ -1011,7 +1043,7 @@ int create(ggb_sa* a, int nodes, int degree, const int* edges, int K, int G, int
   a->K = K;
   a->G = G;
   a->learned = G > K;
-  a->delta = K > 1;
+  a->delta = K > 1 && degree <= 32;   // the endpoint search hands neighbour ids over by warp shuffle
   a->compose_max = compose_max;
   a->n_rand = a->learned ? std::max(1, K / 4) : 0;
   a->C = a->learned ? 4 : 0;
