@@ -46,6 +46,16 @@ struct Swap {
 };
 
 // ---- the base build: one graph, windows split over CTA teams, levels kept ------
+// The base is evaluated with windows of 1024 sources (rows of kBaseR = 8
+// uint4) and keeps every level in the evaluator's own layout
+// [window][level][vertex][8]; its readers serve 128-source sub-windows: sub-
+// window s is chunk s % 8 of window s / 8.
+constexpr int kBaseR = 8;
+
+__device__ __forceinline__ const uint4* sub_row(const uint4* levels, int cap, int N, int s, int k, int v) {
+  return levels + ((((size_t)(s >> 3) * (cap + 1) + k) * N + v) << 3) + (s & 7);
+}
+
 struct BaseResult {
   long long sum;          // the graph's distance sum before + N(N-1)
   int diam;
@@ -61,6 +71,8 @@ struct BaseArgs {
   BaseResult* result;     // written by the launch
   const int* gate;        // the launch does nothing while *gate == 0 (null: always runs)
   int* sticky;            // first error code (never cleared here)
+  long long* sub_counts;  // per 128-source sub-window and level, zeroed here for base_counts_kernel
+  long long sub_count_len;
   int n_teams, team_ctas;
 };
 
@@ -76,6 +88,7 @@ __global__ void __launch_bounds__(kThreads, 1) apsp_base_kernel(ApspArgs a, cons
   const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (a.stats)
     for (long long i = tid; i < (long long)a.N * kStatLevels; i += n_tid) a.stats[i] = 0u;
+  for (long long i = tid; i < b.sub_count_len; i += n_tid) b.sub_counts[i] = 0;
   if (tid == 0) {
     b.result->sum = 0;
     b.result->diam = 1;
@@ -112,37 +125,62 @@ __global__ void __launch_bounds__(kThreads, 1) apsp_base_kernel(ApspArgs a, cons
   }
 }
 
-// ---- per-vertex statistics from the kept levels ------------------------------------
-// stats[v][k] = sum over windows of (l - popc(S_k[v])) for k < kStatLevels:
-// the sources not within distance k of v (the statistics the profile
-// kernel accumulates during its sweeps), read back from the base's rows
-// without atomics.  A block takes 32 vertices (one per lane, so loads are
-// coalesced) and its 8 warps split the windows; the partial sums meet in
-// shared memory.  Levels past a window's completion are full and add
-// nothing.  Runs only while *gate != 0.
+// ---- per-vertex statistics and sub-window counts from the kept levels -------------
+// One pass over the base's rows: stats[v][k] = sum over sub-windows of
+// (l - popc(S_k[v])) for k < kStatLevels (the sources not within distance k
+// of v -- the statistics the profile kernel accumulates during its sweeps),
+// and sub_counts[s][k] = popcount of sub-window s at level k (what the delta
+// evaluation compares against).  A block takes 32 vertices (one per lane: a
+// lane reads its vertex's whole 128-byte row, so a warp's loads are
+// coalesced) and its 8 warps split the windows; statistics meet in shared
+// memory, sub-window counts are warp-reduced and added atomically.  Levels
+// past a window's completion are full and add nothing.  Runs only while
+// *gate != 0.
 constexpr int kStatsWarps = 8;
-__global__ void __launch_bounds__(kStatsWarps * 32) level_stats_kernel(const uint4* __restrict__ levels,
+__global__ void __launch_bounds__(kStatsWarps * 32) base_counts_kernel(const uint4* __restrict__ levels,
                                                                        const int* __restrict__ win_levels, int cap,
-                                                                       int N, int nwin, int n_src,
-                                                                       unsigned* __restrict__ stats, const int* gate) {
+                                                                       int N, int nbw, int n_src,
+                                                                       unsigned* __restrict__ stats,
+                                                                       long long* __restrict__ sub_counts,
+                                                                       const int* gate) {
   __shared__ unsigned s_part[kStatsWarps][kStatLevels][32];
   if (gate && ld_volatile_i32(gate) == 0) return;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int v = blockIdx.x * 32 + lane;
+  const bool live = v < N;
   unsigned acc[kStatLevels];
 #pragma unroll
   for (int k = 0; k < kStatLevels; ++k) acc[k] = 0u;
-  if (v < N) {
-    for (int w = warp; w < nwin; w += kStatsWarps) {
-      const int base = w * 128;
-      const int l = min(128, n_src - base);
-      const int L = win_levels[w];
-      const int top = min(L > 0 ? L : cap, min(cap, kStatLevels - 1));
-      acc[0] += (unsigned)l - ((unsigned)(v - base) < (unsigned)l ? 1u : 0u);
-      const uint4* lev = levels + (size_t)w * (cap + 1) * N + v;
+  for (int t = warp; t < nbw; t += kStatsWarps) {        // warp-uniform
+    int lsub[kBaseR];
+    unsigned lw = 0;
 #pragma unroll
-      for (int k = 1; k < kStatLevels; ++k)
-        if (k <= top) acc[k] += (unsigned)l - popc4(__ldg(lev + (size_t)k * N));
+    for (int c = 0; c < kBaseR; ++c) {
+      lsub[c] = max(0, min(128, n_src - (t * kBaseR + c) * 128));
+      lw += (unsigned)lsub[c];
+    }
+    const int L = win_levels[t];
+    const int top = min(L > 0 ? L : cap, cap);
+    if (live) acc[0] += lw - ((unsigned)(v - t * 1024) < lw ? 1u : 0u);
+#pragma unroll
+    for (int k = 1; k < kStatLevels; ++k) {
+      if (k > top) break;                                  // warp-uniform
+      uint4 r[kBaseR];
+      const uint4* row = levels + (((size_t)t * (cap + 1) + k) * N + (live ? v : 0)) * kBaseR;
+#pragma unroll
+      for (int c = 0; c < kBaseR; ++c) r[c] = live ? __ldg(row + c) : make_uint4(0u, 0u, 0u, 0u);
+      unsigned tot = 0;
+#pragma unroll
+      for (int c = 0; c < kBaseR; ++c) {
+        unsigned pc = popc4(r[c]);
+        tot += pc;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) pc += __shfl_xor_sync(0xffffffffu, pc, o);
+        if (lane == 0 && lsub[c] > 0) atomicAdd(reinterpret_cast<unsigned long long*>(sub_counts) +
+                                                    (size_t)(t * kBaseR + c) * (cap + 1) + k,
+                                                (unsigned long long)pc);
+      }
+      if (live) acc[k] += lw - tot;
     }
   }
 #pragma unroll
@@ -159,6 +197,28 @@ __global__ void __launch_bounds__(kStatsWarps * 32) level_stats_kernel(const uin
   }
 }
 
+// Completion level of every 128-source sub-window: the first level whose
+// count is N * l (the window holding it completed by its own level, so the
+// sub-window did too); level 0's count is l.  -1 or -2 carried over from a
+// window that stalled or ran past the kept levels.  Runs only while *gate != 0.
+__global__ void sub_levels_kernel(long long* __restrict__ sub_counts, const int* __restrict__ win_levels, int cap,
+                                  int N, int nwin, int n_src, int* __restrict__ sub_levels, const int* gate) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nwin) return;
+  if (gate && ld_volatile_i32(gate) == 0) return;
+  const long long l = max(0, min(128, n_src - s * 128));
+  long long* lc = sub_counts + (size_t)s * (cap + 1);
+  lc[0] = l;
+  const int Lp = win_levels[s / kBaseR];
+  int L = Lp;
+  if (Lp >= 0) {
+    L = -1;
+    for (int k = 0; k <= Lp && k <= cap; ++k)
+      if (lc[k] == (long long)N * l) { L = k; break; }
+  }
+  sub_levels[s] = L;
+}
+
 // ---- the delta evaluation: one CTA per (candidate, window), window-major ------------
 constexpr int kDeltaThreads = 256;
 constexpr int kDeltaRows = 512;        // dirty rows a task can hold per level
@@ -167,9 +227,9 @@ constexpr int kDeltaLevels = 48;       // levels a task may run past level 0
 constexpr int kGrp = 8;                // neighbour rows loaded together
 
 struct DeltaArgs {
-  const uint4* levels;                 // base rows, R = 1: [nwin][level_cap + 1][N]
-  const long long* level_counts;       // [nwin][level_cap + 1]
-  const int* win_levels;               // [nwin]
+  const uint4* levels;                 // base rows: [window of 1024][level_cap + 1][N][8] (sub_row)
+  const long long* level_counts;       // [nwin][level_cap + 1] per 128-source sub-window
+  const int* win_levels;               // [nwin] per 128-source sub-window
   const int* adj;                      // base adjacency [N][d]
   const Swap* sw;
   const int* sel;                      // candidate c is sw[sel[c]] (sw[c] when null)
@@ -185,6 +245,12 @@ struct DeltaArgs {
   int N, d, nwin, n_src, level_cap, K;
 };
 
+// a[i] of four values held in registers (a local array indexed at run time
+// would live in local memory)
+__device__ __forceinline__ int pick4(int i, int a0, int a1, int a2, int a3) {
+  return i == 0 ? a0 : i == 1 ? a1 : i == 2 ? a2 : a3;
+}
+
 __device__ __forceinline__ uint4 identity_row(int v, int base, int l) {
   const unsigned b = (unsigned)(v - base);
   uint4 r = make_uint4(0u, 0u, 0u, 0u);
@@ -199,7 +265,7 @@ __device__ __forceinline__ uint4 identity_row(int v, int base, int l) {
   return r;
 }
 
-__global__ void __launch_bounds__(kDeltaThreads) delta_kernel(const DeltaArgs a) {
+__global__ void __launch_bounds__(kDeltaThreads, 4) delta_kernel(const DeltaArgs a) {
   extern __shared__ unsigned s_claim[];                 // [ceil(N/32)]: rows claimed this level, then
                                                         // [ceil(N/32)]: rows in D_k (s_dbits)
   __shared__ int s_ids[2][kDeltaRows];
@@ -208,6 +274,7 @@ __global__ void __launch_bounds__(kDeltaThreads) delta_kernel(const DeltaArgs a)
   __shared__ int s_slot[kDeltaHash];
   __shared__ int s_n[2];
   __shared__ int s_over;
+  __shared__ int s_near;                                // levels 1..s_near are the base's
   __shared__ unsigned long long s_red[kDeltaThreads / 32];
   if (a.stop && ld_volatile_i32(a.stop) != 0) return;
   // window-major: the CTAs resident together share one window's base rows in L2
@@ -230,21 +297,26 @@ __global__ void __launch_bounds__(kDeltaThreads) delta_kernel(const DeltaArgs a)
   // is masked out here and its distances come from endpoint_sweep_kernel.
   // The masked window counts only the other sources: its base counts lose
   // the endpoint's reached vertices, N - stats[x][k] at level k.
+  const int X0 = sw.x[0], X1 = sw.x[1], X2 = sw.x[2], X3 = sw.x[3];
+  const int P0 = sw.pos[0], P1 = sw.pos[1], P2 = sw.pos[2], P3 = sw.pos[3];
   uint4 fullm = chunk_full_mask(0, l);
-  int nmask = 0, mv[4];
+  unsigned mq = 0u;                    // endpoints whose source bit lies in the window
+#pragma unroll
   for (int q = 0; q < 4; ++q) {
     const unsigned b = (unsigned)(sw.x[q] - base);
     if (b < (unsigned)l) {
       const unsigned m = ~(1u << (b & 31));
       if ((b >> 5) == 0) fullm.x &= m; else if ((b >> 5) == 1) fullm.y &= m; else if ((b >> 5) == 2) fullm.z &= m; else fullm.w &= m;
-      mv[nmask++] = sw.x[q];
+      mq |= 1u << q;
     }
   }
-  const int lm = l - nmask;
+  const int lm = l - __popc(mq);
   const long long full_count = (long long)N * lm;
   auto masked_base_count = [&](int k, long long ck) -> long long {
-    for (int i = 0; i < nmask; ++i)
-      ck -= N - (long long)(k < kStatLevels ? __ldg(a.stats + (size_t)mv[i] * kStatLevels + k) : 0u);
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+      if ((mq >> q) & 1u)
+        ck -= N - (long long)(k < kStatLevels ? __ldg(a.stats + (size_t)sw.x[q] * kStatLevels + k) : 0u);
     return ck;
   };
   if (lm == 0) {                       // every source of the window is an endpoint
@@ -255,7 +327,7 @@ __global__ void __launch_bounds__(kDeltaThreads) delta_kernel(const DeltaArgs a)
     return;
   }
   const int cap = a.level_cap;
-  const uint4* const lev = a.levels + (size_t)w * (cap + 1) * N;
+
   const long long* const lc = a.level_counts + (size_t)w * (cap + 1);
   const int nclaim = (N + 31) / 32;
   unsigned* const s_dbits = s_claim + nclaim;
@@ -265,19 +337,18 @@ __global__ void __launch_bounds__(kDeltaThreads) delta_kernel(const DeltaArgs a)
     s_n[0] = 0;
     s_n[1] = 0;
     s_over = 0;
+    s_near = 0x7fffffff;
   }
   __syncthreads();
-  const int X0 = sw.x[0], X1 = sw.x[1], X2 = sw.x[2], X3 = sw.x[3];
-  const int NV[4] = {X2, X3, X0, X1};
   // candidate neighbour j of row x
   auto nb = [&](int x, int j) -> int {
     const int q = x == X0 ? 0 : x == X1 ? 1 : x == X2 ? 2 : x == X3 ? 3 : -1;
-    if (q >= 0 && j == sw.pos[q]) return NV[q];
+    if (q >= 0 && j == pick4(q, P0, P1, P2, P3)) return pick4(q, X2, X3, X0, X1);
     return __ldg(a.adj + (long long)x * d + j);
   };
   auto base_row = [&](int k, int v) -> uint4 {
     if (k > L) return fullm;
-    uint4 r = k == 0 ? identity_row(v, base, l) : __ldg(lev + (size_t)k * N + v);
+    uint4 r = k == 0 ? identity_row(v, base, l) : __ldg(sub_row(a.levels, cap, N, w, k, v));
     r.x &= fullm.x; r.y &= fullm.y; r.z &= fullm.z; r.w &= fullm.w;
     return r;
   };
@@ -299,8 +370,8 @@ __global__ void __launch_bounds__(kDeltaThreads) delta_kernel(const DeltaArgs a)
   // dirty slots (shared memory), then all row loads of a group at once
   auto derive = [&](int k, int nd, int cur, int x) -> uint4 {
     const int qx = x == X0 ? 0 : x == X1 ? 1 : x == X2 ? 2 : x == X3 ? 3 : -1;
-    const int px = qx >= 0 ? sw.pos[qx] : -1;
-    const int vx = qx >= 0 ? NV[qx] : 0;
+    const int px = qx >= 0 ? pick4(qx, P0, P1, P2, P3) : -1;
+    const int vx = pick4(qx, X2, X3, X0, X1);
     const int* row = a.adj + (long long)x * d;
     const int dx = dirty_slot(nd, x);
     uint4 acc = dx >= 0 ? s_val[cur][dx] : base_row(k, x);
@@ -334,21 +405,57 @@ __global__ void __launch_bounds__(kDeltaThreads) delta_kernel(const DeltaArgs a)
     }
     return base_row(k, y);
   };
+  // Levels the candidate shares with the base.  A path of length <= k from
+  // source s that uses a swapped edge reaches an endpoint within k - 1 steps,
+  // so S'_k = S_k for every k <= m = min over the window's (unmasked) sources
+  // of the distance to the nearest endpoint -- the same in both graphs, and
+  // the first level at which some endpoint's base row meets the window.
+  for (int i = threadIdx.x; i < 4 * L; i += blockDim.x) {
+    const uint4 r = base_row(1 + (i >> 2), pick4(i & 3, X0, X1, X2, X3));
+    if (r.x | r.y | r.z | r.w) atomicMin(&s_near, 1 + (i >> 2));
+  }
+  __syncthreads();
+  const int m = s_near <= L ? s_near : 0;
   int cur = 0;
   long long total_delta = 0, prev_count = lm;
   int Lc = -1;
   int status = -2;   // becomes the completion level, or -1 when the candidate stalls
   int k = 0;
   bool dense = false;
+  // The levels past k carry the base's counts (delta 0): the decisions of the
+  // level loop below on those counts.  Returns true once decided.
+  auto base_levels = [&](int k_end) -> bool {
+    for (; k < k_end; ++k) {
+      const long long count = (k + 1 <= L) ? masked_base_count(k + 1, lc[k + 1]) : full_count;
+      if (Lc < 0 && count == full_count) Lc = k + 1;
+      if (Lc >= 0 && k + 1 >= L) { status = Lc; return true; }
+      if (Lc < 0 && count == prev_count) { status = -1; return true; }
+      prev_count = count;
+    }
+    return false;
+  };
+  if (base_levels(m)) k = kDeltaLevels;   // decided within the shared levels
   for (; k < kDeltaLevels; ++k) {
     const int nd = s_n[cur];
+    if (nd == 0) {
+      // S'_k = S_k.  With every endpoint's row full as well, every later
+      // level is the base's too: non-endpoints keep their neighbours, and an
+      // endpoint's row stays full in both graphs.
+      bool all_full = true;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) all_full = all_full && equal4(base_row(k, sw.x[q]), fullm);
+      if (all_full) {
+        base_levels(kDeltaLevels);
+        break;
+      }
+    }
     const int nxt = cur ^ 1;
     const int items = 4 + nd * (d + 1);
     unsigned long long pos_cnt = 0, neg_cnt = 0;
     for (int it = threadIdx.x; it < items; it += blockDim.x) {
       int x;
       if (it < 4) {
-        x = sw.x[it];
+        x = pick4(it, X0, X1, X2, X3);
       } else {
         const int q = (it - 4) / (d + 1), j = (it - 4) % (d + 1);
         const int v = s_ids[cur][q];
@@ -371,17 +478,22 @@ __global__ void __launch_bounds__(kDeltaThreads) delta_kernel(const DeltaArgs a)
       }
     }
     __syncthreads();
-    // clear the claims (every claimed row lies in a word some item touched)
-    for (int it = threadIdx.x; it < items; it += blockDim.x) {
-      int x;
-      if (it < 4) {
-        x = sw.x[it];
-      } else {
-        const int q = (it - 4) / (d + 1), j = (it - 4) % (d + 1);
-        const int v = s_ids[cur][q];
-        x = j == d ? v : nb(v, j);
+    // clear the claims: the whole bitmap when it is small against the items,
+    // else the words the items touched (every claimed row lies in one)
+    if (nclaim <= 2 * items) {
+      for (int i = threadIdx.x; i < nclaim; i += blockDim.x) s_claim[i] = 0u;
+    } else {
+      for (int it = threadIdx.x; it < items; it += blockDim.x) {
+        int x;
+        if (it < 4) {
+          x = pick4(it, X0, X1, X2, X3);
+        } else {
+          const int q = (it - 4) / (d + 1), j = (it - 4) % (d + 1);
+          const int v = s_ids[cur][q];
+          x = j == d ? v : nb(v, j);
+        }
+        s_claim[x >> 5] = 0u;
       }
-      s_claim[x >> 5] = 0u;
     }
     // delta_{k+1} = pos - neg, reduced over the block
     long long dl = (long long)pos_cnt - (long long)neg_cnt;
@@ -435,8 +547,8 @@ __global__ void __launch_bounds__(kDeltaThreads) delta_kernel(const DeltaArgs a)
         for (int v = threadIdx.x; v < N; v += blockDim.x) {
           uint4 acc = __ldcg(A + v);
           const int qv = v == X0 ? 0 : v == X1 ? 1 : v == X2 ? 2 : v == X3 ? 3 : -1;
-          const int pv = qv >= 0 ? sw.pos[qv] : -1;
-          const int nvv = qv >= 0 ? NV[qv] : 0;
+          const int pv = qv >= 0 ? pick4(qv, P0, P1, P2, P3) : -1;
+          const int nvv = pick4(qv, X2, X3, X0, X1);
           const int* row = a.adj + (long long)v * d;
           for (int j0 = 0; j0 < d; j0 += kGrp) {
             int u[kGrp];

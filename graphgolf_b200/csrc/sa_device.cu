@@ -385,9 +385,8 @@ __device__ int base_distance(const uint4* __restrict__ levels, const int* __rest
   const int w = y >> 7, b = y & 127;
   const int L = win_levels[w];
   const int top = L > 0 ? L : cap;
-  const uint4* lev = levels + (size_t)w * (cap + 1) * N + x;
   for (int k = 1; k <= top; ++k) {
-    const uint4 r = __ldg(lev + (size_t)k * N);
+    const uint4 r = __ldg(ggb::sub_row(levels, cap, N, w, k, x));
     const unsigned wd = b < 64 ? (b < 32 ? r.x : r.y) : (b < 96 ? r.z : r.w);
     if ((wd >> (b & 31)) & 1u) return k;
   }
@@ -598,8 +597,11 @@ struct ggb_sa {
   // the base (delta mode): R = 1 windows of the current graph, all levels kept
   int nwin = 0, level_cap = 0, base_T = 0, base_teams = 0;
   uint4* d_levels = nullptr;
-  long long* d_lcounts = nullptr;
-  int* d_winlev = nullptr;
+  int nbw = 0;                        // base windows of 1024 sources
+  long long* d_lcounts = nullptr;     // per 128-source sub-window and level
+  int* d_winlev = nullptr;            // per sub-window completion level
+  long long* d_pcounts = nullptr;     // per base window and level (the build's own bookkeeping)
+  int* d_pwinlev = nullptr;           // per base window completion level
   ggb::ApspCtrl* d_bctrl = nullptr;   // [0]: the grid barrier, [1 + t]: team t
   uint4* d_bscratch = nullptr;
   ggb::BaseResult* d_bres = nullptr;
@@ -704,12 +706,14 @@ int enqueue_profile(ggb_sa* a, const int* gate, cudaStream_t st) {
 int enqueue_base(ggb_sa* a, const int* gate, cudaStream_t st) {
   SCUDA(cudaMemsetAsync(a->d_bctrl, 0, (size_t)(1 + a->base_teams) * sizeof(ggb::ApspCtrl), st));
   ggb::ApspArgs p = graph_args(a);
-  p.stats = nullptr;   // the filter's statistics are read back from the levels (level_stats_kernel)
+  p.stats = nullptr;   // the filter's statistics are read back from the levels (base_counts_kernel)
   p.levels = a->d_levels;
-  p.level_counts = a->d_lcounts;
-  p.win_levels = a->d_winlev;
+  p.level_counts = a->d_pcounts;
+  p.win_levels = a->d_pwinlev;
   p.level_cap = a->level_cap;
   ggb::BaseArgs b;
+  b.sub_counts = a->d_lcounts;
+  b.sub_count_len = (long long)a->nwin * (a->level_cap + 1);
   b.grid_ctrl = a->d_bctrl;
   b.team_ctrl = a->d_bctrl + 1;
   b.scratch = a->d_bscratch;
@@ -719,12 +723,14 @@ int enqueue_base(ggb_sa* a, const int* gate, cudaStream_t st) {
   b.n_teams = a->base_teams;
   b.team_ctas = a->base_T;
   void* params[] = {(void*)&p, (void*)&b};
-  int rc = coop_launch((const void*)ggb::apsp_base_kernel<1>, a->base_teams * a->base_T, ggb::apsp_smem_bytes<1>(),
-                       params, st);
+  int rc = coop_launch((const void*)ggb::apsp_base_kernel<ggb::kBaseR>, a->base_teams * a->base_T,
+                       ggb::apsp_smem_bytes<ggb::kBaseR>(), params, st);
   if (rc) return rc;
-  ggb::level_stats_kernel<<<(a->N + 31) / 32, ggb::kStatsWarps * 32, 0, st>>>(a->d_levels, a->d_winlev, a->level_cap, a->N, a->nwin,
-                                                             a->N, a->d_stats, gate);
-  ggb::core_add_launches(1);
+  ggb::base_counts_kernel<<<(a->N + 31) / 32, ggb::kStatsWarps * 32, 0, st>>>(
+      a->d_levels, a->d_pwinlev, a->level_cap, a->N, a->nbw, a->N, a->d_stats, a->d_lcounts, gate);
+  ggb::sub_levels_kernel<<<(a->nwin + 127) / 128, 128, 0, st>>>(a->d_lcounts, a->d_pwinlev, a->level_cap, a->N,
+                                                               a->nwin, a->N, a->d_winlev, gate);
+  ggb::core_add_launches(2);
   SCUDA(cudaGetLastError());
   return GGB_OK;
 }
@@ -914,7 +920,7 @@ void destroy(ggb_sa* a) {
                   (void*)a->d_sel, (void*)a->d_comp, (void*)a->d_pred, (void*)a->d_vmark, (void*)a->d_labels,
                   (void*)a->d_scores, (void*)a->d_rank, (void*)a->d_rank_key, (void*)a->d_X, (void*)a->d_stats,
                   (void*)a->d_sticky, (void*)a->d_pctrl, (void*)a->d_pbuf, (void*)a->d_levels, (void*)a->d_lcounts,
-                  (void*)a->d_winlev, (void*)a->d_bctrl, (void*)a->d_bscratch, (void*)a->d_bres, (void*)a->d_dsum,
+                  (void*)a->d_winlev, (void*)a->d_pcounts, (void*)a->d_pwinlev, (void*)a->d_bctrl, (void*)a->d_bscratch, (void*)a->d_bres, (void*)a->d_dsum,
                   (void*)a->d_dlev, (void*)a->d_dout, (void*)a->d_dpool, (void*)a->d_dused,
                   (void*)a->d_epsum, (void*)a->d_epecc, (void*)a->d_eprows, (void*)a->d_ephead,
                   (void*)a->d_epnext, (void*)a->d_epmisc, (void*)a->d_epctrl})
@@ -973,19 +979,21 @@ int evaluate_current(ggb_sa* a) {
 
 void set_base_team(ggb_sa* a, int T) {
   a->base_T = T;
-  a->base_teams = std::max(1, std::min(a->sms / T, a->nwin));
+  a->base_teams = std::max(1, std::min(a->sms / T, a->nbw));
 }
 
-// Times the base build of the current graph with teams of 1, 2, 4 and 8 CTAs
-// (two launches each after one warm-up) and keeps the fastest.  The result
-// never depends on the choice.
+// Times the base build of the current graph with teams of 1, 2, 4, 8 and 16
+// CTAs and the size that gives every 1024-source window its own team on the
+// whole GPU (two launches each after one warm-up) and keeps the fastest.  The
+// result never depends on the choice.
 int tune_base(ggb_sa* a) {
   cudaEvent_t e0, e1;
   SCUDA(cudaEventCreate(&e0));
   SCUDA(cudaEventCreate(&e1));
   float best = 1e30f;
   int bestT = 4;
-  for (int T : {1, 2, 4, 8}) {
+  for (int T : {1, 2, 4, 8, 16, std::max(1, a->sms / a->nbw)}) {
+    if (T > a->sms) continue;
     set_base_team(a, T);
     int rc = enqueue_base(a, nullptr, a->st);
     if (rc) return rc;
@@ -1006,19 +1014,21 @@ int tune_base(ggb_sa* a) {
 
 int alloc_base(ggb_sa* a) {
   a->nwin = (a->N + 127) / 128;
+  a->nbw = (a->N + 1023) / 1024;
   // a->level_cap is set by create() from the initial graph's diameter
   set_base_team(a, 1);   // sizes the team arrays for the most teams any plan uses
   int nb = 0;
-  SCUDA(cudaFuncSetAttribute((const void*)ggb::apsp_base_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)ggb::apsp_smem_bytes<1>()));
-  SCUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, (const void*)ggb::apsp_base_kernel<1>, ggb::kThreads,
-                                                      ggb::apsp_smem_bytes<1>()));
+  const void* bk = (const void*)ggb::apsp_base_kernel<ggb::kBaseR>;
+  const size_t bsm = ggb::apsp_smem_bytes<ggb::kBaseR>();
+  SCUDA(cudaFuncSetAttribute(bk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsm));
+  SCUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, bk, ggb::kThreads, bsm));
   if (nb < 1) return core_fail(GGB_ECUDA, "base kernel cannot be resident");
-  const size_t cells = (size_t)a->nwin * (a->level_cap + 1) * a->N;
+  const size_t cells = (size_t)a->nbw * (a->level_cap + 1) * a->N * ggb::kBaseR;
   int rc;
   if ((rc = sdev(&a->d_levels, cells)) || (rc = sdev(&a->d_lcounts, (size_t)a->nwin * (a->level_cap + 1))) ||
-      (rc = sdev(&a->d_winlev, (size_t)a->nwin)) || (rc = sdev(&a->d_bctrl, (size_t)1 + a->base_teams)) ||
-      (rc = sdev(&a->d_bscratch, (size_t)a->base_teams * 2 * a->N)) || (rc = sdev(&a->d_bres, 1)) ||
+      (rc = sdev(&a->d_winlev, (size_t)a->nwin)) || (rc = sdev(&a->d_pcounts, (size_t)a->nbw * (a->level_cap + 1))) ||
+      (rc = sdev(&a->d_pwinlev, (size_t)a->nbw)) || (rc = sdev(&a->d_bctrl, (size_t)1 + a->base_teams)) ||
+      (rc = sdev(&a->d_bscratch, (size_t)a->base_teams * 2 * a->N * ggb::kBaseR)) || (rc = sdev(&a->d_bres, 1)) ||
       (rc = sdev(&a->d_dsum, (size_t)a->K * a->nwin)) || (rc = sdev(&a->d_dlev, (size_t)a->K * a->nwin)) ||
       (rc = sdev(&a->d_dout, (size_t)a->K)))
     return rc;
@@ -1114,7 +1124,7 @@ int create(ggb_sa* a, int nodes, int degree, const int* edges, int K, int G, int
     if ((rc = check_sticky(a))) return rc;
     size_t free_b = 0, total_b = 0;
     SCUDA(cudaMemGetInfo(&free_b, &total_b));
-    const double base_bytes = (double)((nodes + 127) / 128) * (c.diam + 1) * nodes * 16.0;
+    const double base_bytes = (double)((nodes + 1023) / 1024) * 8 * (c.diam + 1) * nodes * 16.0;
     if (c.done && !c.disconnected && c.diam < nodes && base_bytes <= 0.25 * (double)free_b) {
       a->level_cap = std::max(2, c.diam);
       if ((rc = alloc_base(a))) return rc;
