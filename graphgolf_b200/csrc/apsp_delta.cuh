@@ -224,7 +224,7 @@ constexpr int kDeltaThreads = 256;
 constexpr int kDeltaRows = 512;        // dirty rows a task can hold per level
 constexpr int kDeltaHash = 1024;       // hash slots for the dirty rows (power of two)
 constexpr int kDeltaLevels = 48;       // levels a task may run past level 0
-constexpr int kGrp = 8;                // neighbour rows loaded together
+constexpr int kGrp = 6;                // neighbour rows loaded together
 
 struct DeltaArgs {
   const uint4* levels;                 // base rows: [window of 1024][level_cap + 1][N][8] (sub_row)
@@ -366,15 +366,23 @@ __global__ void __launch_bounds__(kDeltaThreads, 4) delta_kernel(const DeltaArgs
     }
     return -1;
   };
+  // this sub-window's rows: level k of vertex v at lev_w + (k * N + v) * 8
+  const uint4* const lev_w = sub_row(a.levels, cap, N, w, 0, 0);
   // S'_{k+1}[x] = S'_k[x] | OR_j S'_k[N'(x)_j]: neighbour ids, then their
-  // dirty slots (shared memory), then all row loads of a group at once
+  // dirty slots (shared memory), then all row loads of a group at once.  The
+  // base rows are ORed unmasked and the mask applied once at the end (the
+  // dirty rows are masked already).
   auto derive = [&](int k, int nd, int cur, int x) -> uint4 {
     const int qx = x == X0 ? 0 : x == X1 ? 1 : x == X2 ? 2 : x == X3 ? 3 : -1;
     const int px = qx >= 0 ? pick4(qx, P0, P1, P2, P3) : -1;
     const int vx = pick4(qx, X2, X3, X0, X1);
     const int* row = a.adj + (long long)x * d;
+    const uint4* const lk = lev_w + (size_t)k * N * 8;
+    auto raw_row = [&](int v) -> uint4 {
+      return k > L ? fullm : (k == 0 ? identity_row(v, base, l) : __ldg(lk + (size_t)v * 8));
+    };
     const int dx = dirty_slot(nd, x);
-    uint4 acc = dx >= 0 ? s_val[cur][dx] : base_row(k, x);
+    uint4 acc = dx >= 0 ? s_val[cur][dx] : raw_row(x);
     for (int j0 = 0; j0 < d; j0 += kGrp) {
       int u[kGrp], ds[kGrp];
 #pragma unroll
@@ -387,10 +395,11 @@ __global__ void __launch_bounds__(kDeltaThreads, 4) delta_kernel(const DeltaArgs
       uint4 r[kGrp];
 #pragma unroll
       for (int q = 0; q < kGrp; ++q)
-        r[q] = u[q] < 0 ? make_uint4(0u, 0u, 0u, 0u) : (ds[q] >= 0 ? s_val[cur][ds[q]] : base_row(k, u[q]));
+        r[q] = u[q] < 0 ? make_uint4(0u, 0u, 0u, 0u) : (ds[q] >= 0 ? s_val[cur][ds[q]] : raw_row(u[q]));
 #pragma unroll
       for (int q = 0; q < kGrp; ++q) or_into(acc, r[q]);
     }
+    acc.x &= fullm.x; acc.y &= fullm.y; acc.z &= fullm.z; acc.w &= fullm.w;
     return acc;
   };
   auto row_k = [&](int k, int nd, int cur, int y) -> uint4 {
@@ -477,7 +486,17 @@ __global__ void __launch_bounds__(kDeltaThreads, 4) delta_kernel(const DeltaArgs
         if (pa > pb) pos_cnt += pa - pb; else neg_cnt += pb - pa;
       }
     }
+    // delta_{k+1} = pos - neg, reduced over the block
+    long long dl = (long long)pos_cnt - (long long)neg_cnt;
+    for (int o = 16; o > 0; o >>= 1) dl += __shfl_xor_sync(0xffffffffu, dl, o);
+    if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = (unsigned long long)dl;
     __syncthreads();
+    // Three barriers a level.  Between the first two, D_k's table is retired
+    // and the claims are cleared; between the second and third, D_{k+1} is
+    // entered.  The next level's items start after the third.
+    if (s_over) { dense = true; break; }   // D_k and its table are still intact
+    long long delta = 0;
+    for (int i = 0; i < kDeltaThreads / 32; ++i) delta += (long long)s_red[i];
     // clear the claims: the whole bitmap when it is small against the items,
     // else the words the items touched (every claimed row lies in one)
     if (nclaim <= 2 * items) {
@@ -495,14 +514,6 @@ __global__ void __launch_bounds__(kDeltaThreads, 4) delta_kernel(const DeltaArgs
         s_claim[x >> 5] = 0u;
       }
     }
-    // delta_{k+1} = pos - neg, reduced over the block
-    long long dl = (long long)pos_cnt - (long long)neg_cnt;
-    for (int o = 16; o > 0; o >>= 1) dl += __shfl_xor_sync(0xffffffffu, dl, o);
-    if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = (unsigned long long)dl;
-    __syncthreads();
-    if (s_over) { dense = true; break; }   // D_k and its table are still intact
-    long long delta = 0;
-    for (int i = 0; i < kDeltaThreads / 32; ++i) delta += (long long)s_red[i];
     // the next level's lookup table and bitmap (every set bit is a D_k row,
     // so clearing the words of D_k's rows clears the bitmap)
     for (int i = threadIdx.x; i < kDeltaHash; i += blockDim.x) s_key[i] = -1;
@@ -516,17 +527,16 @@ __global__ void __launch_bounds__(kDeltaThreads, 4) delta_kernel(const DeltaArgs
       s_slot[h] = i;
       atomicOr(&s_dbits[y >> 5], 1u << (y & 31));
     }
+    if (threadIdx.x == 0) s_n[cur] = 0;    // D_k's count: read before the first barrier only
     total_delta += delta;
     const long long ck = (k + 1 <= L) ? masked_base_count(k + 1, lc[k + 1]) : full_count;
     const long long count = ck + delta;
     if (Lc < 0 && count == full_count) Lc = k + 1;
     __syncthreads();
-    if (threadIdx.x == 0) s_n[cur] = 0;
     if (Lc >= 0 && k + 1 >= L) { status = Lc; break; }
     if (Lc < 0 && count == prev_count) { status = -1; break; }
     prev_count = count;
     cur = nxt;
-    __syncthreads();
   }
   if (dense) {
     // The dirty set outgrew shared memory while deriving level k+1: from
