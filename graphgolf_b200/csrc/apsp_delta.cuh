@@ -130,12 +130,13 @@ __global__ void __launch_bounds__(kThreads, 1) apsp_base_kernel(ApspArgs a, cons
 // (l - popc(S_k[v])) for k < kStatLevels (the sources not within distance k
 // of v -- the statistics the profile kernel accumulates during its sweeps),
 // and sub_counts[s][k] = popcount of sub-window s at level k (what the delta
-// evaluation compares against).  A block takes 32 vertices (one per lane: a
-// lane reads its vertex's whole 128-byte row, so a warp's loads are
-// coalesced) and its 8 warps split the windows; statistics meet in shared
-// memory, sub-window counts are warp-reduced and added atomically.  Levels
-// past a window's completion are full and add nothing.  Runs only while
-// *gate != 0.
+// evaluation compares against).  A block takes 32 vertices, whose rows of one
+// (window, level) are 4 KB of contiguous memory, and its 8 warps split the
+// windows.  A warp reads them in eight 512-byte loads, lane = (row r of four,
+// chunk c): a row's total is reduced over its 8 lanes into shared memory, a
+// chunk's over the lanes holding it and added atomically (lanes 0..7).
+// Levels past a window's completion are full and add nothing.  Runs only
+// while *gate != 0.
 constexpr int kStatsWarps = 8;
 __global__ void __launch_bounds__(kStatsWarps * 32) base_counts_kernel(const uint4* __restrict__ levels,
                                                                        const int* __restrict__ win_levels, int cap,
@@ -143,52 +144,52 @@ __global__ void __launch_bounds__(kStatsWarps * 32) base_counts_kernel(const uin
                                                                        unsigned* __restrict__ stats,
                                                                        long long* __restrict__ sub_counts,
                                                                        const int* gate) {
+  static_assert(kBaseR == 8, "a lane reads one 16-byte chunk of a 128-byte row");
   __shared__ unsigned s_part[kStatsWarps][kStatLevels][32];
   if (gate && ld_volatile_i32(gate) == 0) return;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int v = blockIdx.x * 32 + lane;
-  const bool live = v < N;
-  unsigned acc[kStatLevels];
-#pragma unroll
-  for (int k = 0; k < kStatLevels; ++k) acc[k] = 0u;
+  const int c = lane & 7, rl = lane >> 3;
+  const int v0 = blockIdx.x * 32;
+  for (int i = lane; i < kStatLevels * 32; i += 32) (&s_part[warp][0][0])[i] = 0u;
+  __syncwarp();
   for (int t = warp; t < nbw; t += kStatsWarps) {        // warp-uniform
-    int lsub[kBaseR];
-    unsigned lw = 0;
-#pragma unroll
-    for (int c = 0; c < kBaseR; ++c) {
-      lsub[c] = max(0, min(128, n_src - (t * kBaseR + c) * 128));
-      lw += (unsigned)lsub[c];
-    }
+    const int lsub = max(0, min(128, n_src - (t * kBaseR + c) * 128));   // sources of chunk c
+    const unsigned lw = (unsigned)max(0, min(128 * kBaseR, n_src - t * 128 * kBaseR));
     const int L = win_levels[t];
     const int top = min(L > 0 ? L : cap, cap);
-    if (live) acc[0] += lw - ((unsigned)(v - t * 1024) < lw ? 1u : 0u);
+    if (v0 + lane < N) s_part[warp][0][lane] += lw - ((unsigned)(v0 + lane - t * 128 * kBaseR) < lw ? 1u : 0u);
+    for (int k = 1; k <= top; ++k) {                     // counts of every kept level
+      const bool stat = k < kStatLevels;                   // statistics of the first 32
+      const uint4* rows = levels + (((size_t)t * (cap + 1) + k) * N + v0) * kBaseR;
+      uint4 x[8];
 #pragma unroll
-    for (int k = 1; k < kStatLevels; ++k) {
-      if (k > top) break;                                  // warp-uniform
-      uint4 r[kBaseR];
-      const uint4* row = levels + (((size_t)t * (cap + 1) + k) * N + (live ? v : 0)) * kBaseR;
-#pragma unroll
-      for (int c = 0; c < kBaseR; ++c) r[c] = live ? __ldg(row + c) : make_uint4(0u, 0u, 0u, 0u);
-      unsigned tot = 0;
-#pragma unroll
-      for (int c = 0; c < kBaseR; ++c) {
-        unsigned pc = popc4(r[c]);
-        tot += pc;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) pc += __shfl_xor_sync(0xffffffffu, pc, o);
-        if (lane == 0 && lsub[c] > 0) atomicAdd(reinterpret_cast<unsigned long long*>(sub_counts) +
-                                                    (size_t)(t * kBaseR + c) * (cap + 1) + k,
-                                                (unsigned long long)pc);
+      for (int i = 0; i < 8; ++i) {
+        const int r = 4 * i + rl;
+        x[i] = v0 + r < N ? __ldg(rows + r * kBaseR + c) : make_uint4(0u, 0u, 0u, 0u);
       }
-      if (live) acc[k] += lw - tot;
+      unsigned csum = 0;
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const int r = 4 * i + rl;
+        const unsigned pc = popc4(x[i]);
+        csum += pc;
+        unsigned rs = pc;
+        rs += __shfl_xor_sync(0xffffffffu, rs, 1);
+        rs += __shfl_xor_sync(0xffffffffu, rs, 2);
+        rs += __shfl_xor_sync(0xffffffffu, rs, 4);
+        if (stat && c == 0 && v0 + r < N) s_part[warp][k][r] += lw - rs;
+      }
+      csum += __shfl_xor_sync(0xffffffffu, csum, 8);
+      csum += __shfl_xor_sync(0xffffffffu, csum, 16);
+      if (lane < 8 && lsub > 0)
+        atomicAdd(reinterpret_cast<unsigned long long*>(sub_counts) + (size_t)(t * kBaseR + c) * (cap + 1) + k,
+                  (unsigned long long)csum);
     }
   }
-#pragma unroll
-  for (int k = 0; k < kStatLevels; ++k) s_part[warp][k][lane] = acc[k];
   __syncthreads();
   for (int i = threadIdx.x; i < 32 * kStatLevels; i += blockDim.x) {
     const int vl = i / kStatLevels, k = i % kStatLevels;
-    const int vv = blockIdx.x * 32 + vl;
+    const int vv = v0 + vl;
     if (vv >= N) continue;
     unsigned t = 0u;
 #pragma unroll
@@ -761,6 +762,10 @@ __global__ void delta_reduce_kernel(const DeltaArgs a, const BaseResult* __restr
     if (e == -1) stalled = 1;
     else if (e < 0) missing = 1;
     else mx = max(mx, e);
+    // The statistics keep kStatLevels levels: an endpoint that reaches past
+    // them in the base has neither its transmission nor (in the windows that
+    // mask it) its reached counts there.  Such a candidate is not served.
+    if (st[kStatLevels - 1] != 0u) missing = 1;
   }
   for (int w = lane; w < a.nwin; w += 32) {
     s += a.dsum[(size_t)c * a.nwin + w];

@@ -75,6 +75,55 @@ def test_large_diameter_graph(gpu):
         _check(an, g, st)
 
 
+def _ladder(rungs):
+    """A ladder of `rungs` rungs closed at each end by a K4 less one edge:
+    3-regular and path-like (diameter about rungs + 3), its middle vertices of
+    eccentricity about half of that."""
+    e = []
+    for i in range(rungs):
+        e.append((i, rungs + i))
+        if i + 1 < rungs:
+            e += [(i, i + 1), (rungs + i, rungs + i + 1)]
+    n = 2 * rungs
+    for o, m in [(0, rungs), (rungs - 1, 2 * rungs - 1)]:
+        p, q, r, s = n, n + 1, n + 2, n + 3
+        e += [(p, r), (p, s), (q, r), (q, s), (r, s), (o, p), (m, q)]
+        n += 4
+    e = np.array(e, dtype=np.int32)
+    return graphs.Graph(n, 3, e, graphs.create_adj(n, 3, e))
+
+
+def _prism(k):
+    """Two k-cycles joined by spokes: 3-regular, every eccentricity k/2 + 1."""
+    e = [(i, (i + 1) % k) for i in range(k)] + [(k + i, k + (i + 1) % k) for i in range(k)] + \
+        [(i, k + i) for i in range(k)]
+    e = np.array(e, dtype=np.int32)
+    return graphs.Graph(2 * k, 3, e, graphs.create_adj(2 * k, 3, e))
+
+
+def test_levels_past_the_statistics(gpu):
+    """The per-vertex statistics keep 32 levels.  A ladder of diameter about
+    39: the base keeps every level, and candidates whose endpoints all lie
+    within 31 of every vertex are served on levels past 32 and equal their
+    full evaluation; the others are not served, never wrong.  A prism whose
+    every eccentricity is 33: no candidate is served, so the annealer
+    evaluates in full."""
+    g = _ladder(36)
+    assert 33 <= gg.evaluate(g.adj).diameter <= 45
+    with gg.Annealer(g, candidates=128, compose=8, seed=4) as an:
+        c, m, u = an.check_delta()
+        assert m == 0 and c + u == 128 and c > 0
+        _check(an, g, an.run(3))
+    g = _prism(64)
+    assert gg.evaluate(g.adj).diameter == 33
+    with gg.Annealer(g, candidates=16, compose=4, seed=5) as an:
+        c, m, u = an.check_delta()
+        assert m == 0 and c == 0 and u == 16
+        st = an.run(3)
+        assert not st.delta
+        _check(an, g, st)
+
+
 def test_metropolis_states_exact(gpu):
     g = graphs.random_regular(400, 5, 4)
     with gg.Annealer(g, candidates=4, seed=9) as an:
