@@ -285,10 +285,11 @@ __device__ __forceinline__ void set_bit_in(unsigned* row, int x, int base, int n
 // longer rows are taken one at a time.  Up to 8 loads are in flight per lane
 // and the bit sets are predicated, not branched.  With out_ids, entry e of
 // row j is also stored at out_ids[j*d + e] (-1 for an invalid row id).
-// Per-lane count of newly set bits by window, in shared memory: lane L owns
-// the column col = base + L of a [window][32] array, so counting never
-// conflicts or needs an atomic.  Bit b lies in global window b >> log2w; only
-// this rank's windows (first, first + stride, ...) are counted.
+// The warp's count of newly set bits by window, in shared memory (one
+// counter per window, shared atomics: only the d + d^2 bits of the first two
+// steps are counted, and a per-lane array would cost the occupancy of a CTA
+// per SM).  Bit b lies in global window b >> log2w; only this rank's windows
+// (first, first + stride, ...) are counted.
 struct NewBitCount {
   unsigned* col;
   int log2w, first, stride, nwin;
@@ -299,7 +300,7 @@ struct NewBitCount {
       if (k % stride) return;
       k /= stride;
     }
-    if (k < nwin) col[k * 32] += 1u;
+    if (k < nwin) atomicAdd(col + k, 1u);
   }
 };
 
@@ -482,10 +483,10 @@ struct BallArgs {
 __host__ __device__ __forceinline__ int ball_row_u4(int n_src) { return ((n_src + 127) / 128 + 3) / 4 * 4; }
 
 // Shared memory of one warp of ball_kernel, in uint4: the full row, the one-
-// and two-hop neighbour ids (d + d^2 ints, padded) and the per-lane new-bit
+// and two-hop neighbour ids (d + d^2 ints, padded) and the warp's new-bit
 // counters of S_1 and S_2 for nwin windows.
 __host__ __device__ __forceinline__ int ball_warp_u4(int n_src, int d, int nwin) {
-  return ball_row_u4(n_src) + (d + d * d + 3) / 4 + 2 * nwin * 32 / 4;
+  return ball_row_u4(n_src) + (d + d * d + 3) / 4 + (2 * nwin + 3) / 4;
 }
 
 // The ball pre-pass runs only without added centres (every row is a "lo"
@@ -494,7 +495,7 @@ __host__ __device__ __forceinline__ int ball_warp_u4(int n_src, int d, int nwin)
 // count of S_3 is taken by the window's first dense sweep, which reads every
 // S_3 row anyway.
 template <int VEC>
-__global__ void __launch_bounds__(kBallThreads, 2) ball_kernel(const BallArgs b) {
+__global__ void __launch_bounds__(kBallThreads, 3) ball_kernel(const BallArgs b) {
   extern __shared__ uint4 s_ball[];
   constexpr int kWarpsB = kBallThreads / 32;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -505,12 +506,12 @@ __global__ void __launch_bounds__(kBallThreads, 2) ball_kernel(const BallArgs b)
   unsigned* const row = reinterpret_cast<unsigned*>(row4);
   int* const nb1 = reinterpret_cast<int*>(row4 + row_u4);
   int* const nb2 = nb1 + d;
-  unsigned* const lc = reinterpret_cast<unsigned*>(row4 + row_u4 + (d + d * d + 3) / 4);  // [2][nwin][32]
-  for (int i = lane; i < 2 * nwin * 32; i += 32) lc[i] = 0u;
+  unsigned* const lc = reinterpret_cast<unsigned*>(row4 + row_u4 + (d + d * d + 3) / 4);  // [2][nwin]
+  for (int i = lane; i < 2 * nwin; i += 32) lc[i] = 0u;
   int log2w = 0;
   while ((128 * R) >> log2w > 1) ++log2w;
-  const NewBitCount c1{lc + lane, log2w, b.win_first, b.win_stride, nwin};
-  const NewBitCount c2{lc + nwin * 32 + lane, log2w, b.win_first, b.win_stride, nwin};
+  const NewBitCount c1{lc, log2w, b.win_first, b.win_stride, nwin};
+  const NewBitCount c2{lc + nwin, log2w, b.win_first, b.win_stride, nwin};
   bool adj_ok = true;
   const long long warp_id = (long long)blockIdx.x * kWarpsB + warp;
   const long long n_warps = (long long)gridDim.x * kWarpsB;
@@ -543,13 +544,10 @@ __global__ void __launch_bounds__(kBallThreads, 2) ball_kernel(const BallArgs b)
     __syncwarp();
   }
   if (!adj_ok) set_error(b.ctrl, kErrAdj, (int)blockIdx.x);
-  // lane k sums window k's columns: S_1 = new bits of step 1, S_2 = S_1 + new bits of step 2
+  // lane k adds window k's counts: S_1 = new bits of step 1, S_2 = S_1 + new bits of step 2
+  __syncwarp();
   if (lane < nwin) {
-    unsigned long long s1 = 0, s2 = 0;
-    for (int i = 0; i < 32; ++i) {
-      s1 += lc[lane * 32 + i];
-      s2 += lc[nwin * 32 + lane * 32 + i];
-    }
+    const unsigned long long s1 = lc[lane], s2 = lc[nwin + lane];
     if (s1) atomicAdd(b.cnt + (size_t)lane * 6 + 0, s1);
     if (s1 + s2) atomicAdd(b.cnt + (size_t)lane * 6 + 2, s1 + s2);
   }
