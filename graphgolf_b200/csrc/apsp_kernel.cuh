@@ -247,11 +247,13 @@ template <int VEC> struct AdjVec;
 template <> struct AdjVec<1> {
   int v;
   __device__ __forceinline__ void load(const int* p) { v = __ldg(p); }
+  __device__ __forceinline__ void fill(int x) { v = x; }
   __device__ __forceinline__ int at(int) const { return v; }
 };
 template <> struct AdjVec<4> {
   int4 v;
   __device__ __forceinline__ void load(const int* p) { v = __ldg(reinterpret_cast<const int4*>(p)); }
+  __device__ __forceinline__ void fill(int x) { v = make_int4(x, x, x, x); }
   __device__ __forceinline__ int at(int i) const { return i == 0 ? v.x : i == 1 ? v.y : i == 2 ? v.z : v.w; }
 };
 
@@ -459,6 +461,40 @@ __device__ __forceinline__ void seed_window(const ApspArgs& a, const int* __rest
   }
 }
 
+// The ball's last step: OR into `row` the bit of every entry below nbits of
+// the rows ids[0..nrows), d / VEC <= 32 lanes a row, 8 loads in flight per
+// lane.  A row id outside [0, N) is skipped and so is an entry outside
+// [0, nbits); neither is reported here, because the ball's first step reads
+// every row of the adjacency and reports any entry outside [0, N).  One
+// compare, two shifts, an add and the shared reduction per entry.
+template <int VEC>
+__device__ __forceinline__ void scatter_plain(const int* __restrict__ adj, int N, int d, const int* ids, int nrows,
+                                              unsigned* row, int nbits, int lane) {
+  const unsigned rs = (unsigned)__cvta_generic_to_shared(row);
+  const int per = d / VEC;
+  const int rpi = 32 / per;
+  const int roff = lane / per, part = lane - roff * per;
+  const bool active = roff < rpi;
+  for (int r0 = 0; r0 < nrows; r0 += rpi * 8) {
+    AdjVec<VEC> val[8];
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+      const int j = r0 + t * rpi + roff;
+      const int u = (active && j < nrows) ? ids[j] : -1;
+      if ((unsigned)u < (unsigned)N) val[t].load(adj + (long long)u * d + part * VEC);
+      else val[t].fill(-1);
+    }
+#pragma unroll
+    for (int t = 0; t < 8; ++t)
+#pragma unroll
+      for (int e = 0; e < VEC; ++e) {
+        const unsigned x = (unsigned)val[t].at(e);
+        if (x < (unsigned)nbits)
+          asm volatile("red.shared.or.b32 [%0], %1;" ::"r"(rs + ((x >> 5) << 2)), "r"(1u << (x & 31)) : "memory");
+      }
+  }
+}
+
 // ---- the ball pre-pass: S_3 of every window at once --------------------------
 //
 // One warp per vertex v builds, in shared memory, the row of all phase-1
@@ -531,7 +567,10 @@ __global__ void __launch_bounds__(kBallThreads, 3) ball_kernel(const BallArgs b)
     set_rows_bits<VEC, 32>(b.adj, N, d, nb1, d, row, 0, b.n_src, lane, adj_ok, nb2, &c2);
     __syncwarp();
     // S_3 = S_2 u N(N(N(v)))
-    set_rows_bits<VEC, 32>(b.adj, N, d, nb2, d * d, row, 0, b.n_src, lane, adj_ok, nullptr, nullptr);
+    if (d / VEC <= 32)
+      scatter_plain<VEC>(b.adj, N, d, nb2, d * d, row, b.n_src, lane);
+    else
+      set_rows_bits<VEC, 32>(b.adj, N, d, nb2, d * d, row, 0, b.n_src, lane, adj_ok, nullptr, nullptr);
     __syncwarp();
     for (int k = 0; k < nwin; ++k) {
       const int t = b.win_first + k * b.win_stride;
