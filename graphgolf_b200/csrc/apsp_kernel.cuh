@@ -154,6 +154,18 @@ __device__ __forceinline__ bool grid_barrier(ApspCtrl* c, unsigned long long tar
 
 __device__ __forceinline__ uint4 ld_cg(const uint4* p) { return __ldcg(p); }
 __device__ __forceinline__ void st_cg(uint4* p, const uint4& v) { __stcg(p, v); }
+// 32 bytes (two adjacent uint4, 32-byte aligned) in one L2-cached access
+__device__ __forceinline__ void ld_cg2(const uint4* p, uint4 (&v)[2]) {
+  asm volatile("ld.global.cg.v8.u32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+               : "=r"(v[0].x), "=r"(v[0].y), "=r"(v[0].z), "=r"(v[0].w), "=r"(v[1].x), "=r"(v[1].y), "=r"(v[1].z),
+                 "=r"(v[1].w)
+               : "l"(p));
+}
+__device__ __forceinline__ void st_cg2(uint4* p, const uint4 (&v)[2]) {
+  asm volatile("st.global.cg.v8.u32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"l"(p), "r"(v[0].x), "r"(v[0].y),
+               "r"(v[0].z), "r"(v[0].w), "r"(v[1].x), "r"(v[1].y), "r"(v[1].z), "r"(v[1].w)
+               : "memory");
+}
 
 __device__ __forceinline__ void or_into(uint4& a, const uint4& b) {
   a.x |= b.x; a.y |= b.y; a.z |= b.z; a.w |= b.w;
@@ -852,6 +864,62 @@ __device__ __forceinline__ bool eval_windows(const ApspArgs& a, int cta, int nct
                                    a.stats, (int)kk + 1);
             }
           }
+          if constexpr (R == 32) {
+            // 32-byte accesses: a half-warp per row, two rows per warp step
+            // (vertex v of the step and the one n_slots further)
+            const int h = lane >> 4, hl = lane & 15;
+            constexpr int U2 = 8;
+            for (long long vb = wide ? N : slot; vb < N; vb += 2 * n_slots) {
+              const long long v = vb + h * n_slots;
+              const bool live = v < N;
+              const long long vv = live ? v : vb;   // a dead half reads a live row and drops the result
+              const int* arow = adjp + vv * d;
+              uint4 acc[2];
+              ld_cg2(src + vv * R + 2 * hl, acc);
+              if (own_count && live) {
+                const unsigned co = popc4(acc[0]) + popc4(acc[1]);
+                if (v < a.split) cl[2] += co; else cl[3] += co;
+              }
+              int j = 0;
+              for (; j + U2 <= d; j += U2) {
+                int u[U2];
+#pragma unroll
+                for (int q = 0; q < U2; ++q) u[q] = __ldg(arow + j + q);
+#pragma unroll
+                for (int q = 0; q < U2; ++q) {
+                  if ((unsigned)u[q] >= (unsigned)N) { adj_ok = false; u[q] = 0; }
+                }
+                uint4 x[U2][2];
+#pragma unroll
+                for (int q = 0; q < U2; ++q) ld_cg2(src + (long long)u[q] * R + 2 * hl, x[q]);
+#pragma unroll
+                for (int q = 0; q < U2; ++q) {
+                  or_into(acc[0], x[q][0]);
+                  or_into(acc[1], x[q][1]);
+                }
+              }
+              for (; j < d; ++j) {
+                int u = __ldg(arow + j);
+                if ((unsigned)u >= (unsigned)N) { adj_ok = false; u = 0; }
+                uint4 x[2];
+                ld_cg2(src + (long long)u * R + 2 * hl, x);
+                or_into(acc[0], x[0]);
+                or_into(acc[1], x[1]);
+              }
+              const unsigned cc = live ? popc4(acc[0]) + popc4(acc[1]) : 0u;
+              if (live) {
+                st_cg2(dst + v * R + 2 * hl, acc);
+                if (v < a.split) cl[0] += cc; else cl[1] += cc;
+              }
+              if constexpr (STATS) {
+                unsigned tot = cc;
+#pragma unroll
+                for (int o = 8; o > 0; o >>= 1) tot += __shfl_xor_sync(0xffffffffu, tot, o);
+                if (live && hl == 0 && kk + 1 < kStatLevels)
+                  atomicAdd(a.stats + v * kStatLevels + kk + 1, (unsigned)l - tot);
+              }
+            }
+          } else
           for (long long v = wide ? N : slot; v < N; v += n_slots) {
             const int* arow = adjp + v * d;
             uint4 acc[UPL];
