@@ -710,6 +710,82 @@ __device__ __forceinline__ void sweep_wide(const uint4* __restrict__ src, uint4*
   }
 }
 
+// The same sweep for rows of 32 uint4 and degree d <= 16 with 32-byte
+// accesses: a half-warp per row (lane hl owns uint4 2hl and 2hl + 1), two
+// rows per warp step (vertex v and the one `stride` further).  Lane hl < d
+// of a half holds neighbour hl of its vertex; the next step's ids and own
+// rows are loaded while the current gathers are in flight; a lane whose 32
+// bytes are full loads nothing, checked again after every group of 8
+// neighbour rows.
+template <int R, bool STATS = false>
+__device__ __forceinline__ void sweep_wide_half(const uint4* __restrict__ src, uint4* __restrict__ dst,
+                                                const int* __restrict__ adj, int N, int d, int split, long long v0,
+                                                long long stride, int l, unsigned (&cl)[4], bool& adj_ok,
+                                                unsigned* stats = nullptr, int lvl = 0) {
+  static_assert(R == 32, "two uint4 of the row a lane");
+  constexpr int U = 4;
+  const int lane = threadIdx.x & 31, h = lane >> 4, hl = lane & 15;
+  const uint4 zero = make_uint4(0u, 0u, 0u, 0u);
+  const uint4 fm[2] = {chunk_full_mask(2 * hl, l), chunk_full_mask(2 * hl + 1, l)};
+  auto full = [&](const uint4 (&r)[2]) { return equal4(r[0], fm[0]) && equal4(r[1], fm[1]); };
+  // ids and own row of this half's vertex of the step at vb (past N: a full
+  // row, so nothing is gathered for it)
+  auto fetch = [&](long long vb, int& ids, uint4 (&own)[2]) {
+    const long long v = vb + h * stride;
+    if (v < N) {
+      ids = hl < d ? __ldg(adj + v * d + hl) : 0;
+      ld_cg2(src + v * R + 2 * hl, own);
+    } else {
+      ids = 0;
+      own[0] = fm[0];
+      own[1] = fm[1];
+    }
+  };
+  int u_nx;
+  uint4 own_nx[2];
+  fetch(v0, u_nx, own_nx);
+  for (long long vb = v0; vb < N; vb += 2 * stride) {
+    const long long v = vb + h * stride;
+    const bool live = v < N;
+    int u_me = u_nx;
+    uint4 acc[2] = {own_nx[0], own_nx[1]};
+    fetch(vb + 2 * stride, u_nx, own_nx);
+    if (hl < d && (unsigned)u_me >= (unsigned)N) { adj_ok = false; u_me = 0; }
+    bool need = live && !full(acc);
+    for (int j0 = 0; j0 < d; j0 += U) {
+      uint4 x[U][2];
+#pragma unroll
+      for (int q = 0; q < U; ++q) {
+        const int j = j0 + q;
+        const int u = __shfl_sync(0xffffffffu, u_me, (h << 4) | (j & 15));
+        if (j < d && need) {
+          ld_cg2(src + (long long)u * R + 2 * hl, x[q]);
+        } else {
+          x[q][0] = zero;
+          x[q][1] = zero;
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < U; ++q) {
+        or_into(acc[0], x[q][0]);
+        or_into(acc[1], x[q][1]);
+      }
+      need = live && !full(acc);
+    }
+    const unsigned cc = live ? popc4(acc[0]) + popc4(acc[1]) : 0u;
+    if (live) {
+      st_cg2(dst + v * R + 2 * hl, acc);
+      if (v < split) cl[0] += cc; else cl[1] += cc;
+    }
+    if constexpr (STATS) {
+      unsigned tot = cc;
+#pragma unroll
+      for (int o = 8; o > 0; o >>= 1) tot += __shfl_xor_sync(0xffffffffu, tot, o);
+      if (live && hl == 0 && lvl < kStatLevels) atomicAdd(stats + v * kStatLevels + lvl, (unsigned)l - tot);
+    }
+  }
+}
+
 // ---- one graph on a team of CTAs ------------------------------------------------
 // R = uint4 words per row (W = 128*R source bits).  LPR lanes share a row,
 // each lane owning UPL uint4 of it; a warp covers VPW vertices per step.
@@ -860,8 +936,17 @@ __device__ __forceinline__ bool eval_windows(const ApspArgs& a, int cta, int nct
           if constexpr (LPR == 32) {
             if (d <= 32 && !own_count && prev_total * 10 >= (long long)N * l * 9) {
               wide = true;
-              sweep_wide<R, STATS>(src, dst, adjp, N, d, a.split, slot, n_slots, l, own_count, cl, adj_ok,
-                                   a.stats, (int)kk + 1);
+              bool half = false;
+              if constexpr (R == 32) {
+                if (d <= 16) {
+                  half = true;
+                  sweep_wide_half<R, STATS>(src, dst, adjp, N, d, a.split, slot, n_slots, l, cl, adj_ok, a.stats,
+                                            (int)kk + 1);
+                }
+              }
+              if (!half)
+                sweep_wide<R, STATS>(src, dst, adjp, N, d, a.split, slot, n_slots, l, own_count, cl, adj_ok,
+                                     a.stats, (int)kk + 1);
             }
           }
           if constexpr (R == 32) {
