@@ -949,20 +949,27 @@ __device__ __forceinline__ bool eval_windows(const ApspArgs& a, int cta, int nct
                                      a.stats, (int)kk + 1);
             }
           }
-          if constexpr (R == 32) {
-            // 32-byte accesses: a half-warp per row, two rows per warp step
-            // (vertex v of the step and the one n_slots further)
-            const int h = lane >> 4, hl = lane & 15;
-            constexpr int U2 = 8;
+          if constexpr (R >= 8) {
+            // 32-byte accesses: each group of LPR lanes serves two rows, LP
+            // lanes a row, PPL 32-byte parts a lane (vertex v of the step and
+            // the one n_slots further); half the load instructions of
+            // 16-byte accesses
+            constexpr int LP = LPR / 2;
+            constexpr int PPL = R / (2 * LP);
+            constexpr int U2 = 8 / PPL;
+            const int h = li / LP, hl = li % LP;
             for (long long vb = wide ? N : slot; vb < N; vb += 2 * n_slots) {
               const long long v = vb + h * n_slots;
               const bool live = v < N;
               const long long vv = live ? v : vb;   // a dead half reads a live row and drops the result
               const int* arow = adjp + vv * d;
-              uint4 acc[2];
-              ld_cg2(src + vv * R + 2 * hl, acc);
+              uint4 acc[PPL][2];
+#pragma unroll
+              for (int p = 0; p < PPL; ++p) ld_cg2(src + vv * R + 2 * (hl + p * LP), acc[p]);
               if (own_count && live) {
-                const unsigned co = popc4(acc[0]) + popc4(acc[1]);
+                unsigned co = 0;
+#pragma unroll
+                for (int p = 0; p < PPL; ++p) co += popc4(acc[p][0]) + popc4(acc[p][1]);
                 if (v < a.split) cl[2] += co; else cl[3] += co;
               }
               int j = 0;
@@ -974,32 +981,44 @@ __device__ __forceinline__ bool eval_windows(const ApspArgs& a, int cta, int nct
                 for (int q = 0; q < U2; ++q) {
                   if ((unsigned)u[q] >= (unsigned)N) { adj_ok = false; u[q] = 0; }
                 }
-                uint4 x[U2][2];
+                uint4 x[U2][PPL][2];
 #pragma unroll
-                for (int q = 0; q < U2; ++q) ld_cg2(src + (long long)u[q] * R + 2 * hl, x[q]);
+                for (int q = 0; q < U2; ++q)
 #pragma unroll
-                for (int q = 0; q < U2; ++q) {
-                  or_into(acc[0], x[q][0]);
-                  or_into(acc[1], x[q][1]);
-                }
+                  for (int p = 0; p < PPL; ++p) ld_cg2(src + (long long)u[q] * R + 2 * (hl + p * LP), x[q][p]);
+#pragma unroll
+                for (int q = 0; q < U2; ++q)
+#pragma unroll
+                  for (int p = 0; p < PPL; ++p) {
+                    or_into(acc[p][0], x[q][p][0]);
+                    or_into(acc[p][1], x[q][p][1]);
+                  }
               }
               for (; j < d; ++j) {
                 int u = __ldg(arow + j);
                 if ((unsigned)u >= (unsigned)N) { adj_ok = false; u = 0; }
-                uint4 x[2];
-                ld_cg2(src + (long long)u * R + 2 * hl, x);
-                or_into(acc[0], x[0]);
-                or_into(acc[1], x[1]);
+#pragma unroll
+                for (int p = 0; p < PPL; ++p) {
+                  uint4 x[2];
+                  ld_cg2(src + (long long)u * R + 2 * (hl + p * LP), x);
+                  or_into(acc[p][0], x[0]);
+                  or_into(acc[p][1], x[1]);
+                }
               }
-              const unsigned cc = live ? popc4(acc[0]) + popc4(acc[1]) : 0u;
+              unsigned cc = 0;
               if (live) {
-                st_cg2(dst + v * R + 2 * hl, acc);
+#pragma unroll
+                for (int p = 0; p < PPL; ++p) {
+                  st_cg2(dst + v * R + 2 * (hl + p * LP), acc[p]);
+                  cc += popc4(acc[p][0]) + popc4(acc[p][1]);
+                }
                 if (v < a.split) cl[0] += cc; else cl[1] += cc;
               }
               if constexpr (STATS) {
+                // the LP lanes of this row hold its popcount in parts
                 unsigned tot = cc;
 #pragma unroll
-                for (int o = 8; o > 0; o >>= 1) tot += __shfl_xor_sync(0xffffffffu, tot, o);
+                for (int o = LP / 2; o > 0; o >>= 1) tot += __shfl_xor_sync(0xffffffffu, tot, o);
                 if (live && hl == 0 && kk + 1 < kStatLevels)
                   atomicAdd(a.stats + v * kStatLevels + kk + 1, (unsigned)l - tot);
               }
