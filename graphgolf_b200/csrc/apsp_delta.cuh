@@ -386,10 +386,25 @@ __global__ void __launch_bounds__(kDeltaThreads, 4) delta_kernel(const DeltaArgs
     uint4 acc = dx >= 0 ? s_val[cur][dx] : raw_row(x);
     for (int j0 = 0; j0 < d; j0 += kGrp) {
       int u[kGrp], ds[kGrp];
+      if ((d & 1) == 0) {                // pairs of ids in one 8-byte load (x * d + j is even)
 #pragma unroll
-      for (int q = 0; q < kGrp; ++q) {
-        const int j = j0 + q;
-        u[q] = j < d ? (j == px ? vx : __ldg(row + j)) : -1;
+        for (int q = 0; q < kGrp; q += 2) {
+          const int j = j0 + q;
+          if (j < d) {
+            const int2 t = __ldg(reinterpret_cast<const int2*>(row + j));
+            u[q] = j == px ? vx : t.x;
+            u[q + 1] = j + 1 == px ? vx : t.y;
+          } else {
+            u[q] = -1;
+            u[q + 1] = -1;
+          }
+        }
+      } else {
+#pragma unroll
+        for (int q = 0; q < kGrp; ++q) {
+          const int j = j0 + q;
+          u[q] = j < d ? (j == px ? vx : __ldg(row + j)) : -1;
+        }
       }
 #pragma unroll
       for (int q = 0; q < kGrp; ++q) ds[q] = u[q] >= 0 ? dirty_slot(nd, u[q]) : -1;
