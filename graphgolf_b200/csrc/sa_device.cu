@@ -594,7 +594,8 @@ struct ggb_sa {
   int pR = 0;
   ggb::ApspCtrl* d_pctrl = nullptr;
   uint4* d_pbuf = nullptr;
-  // the base (delta mode): R = 1 windows of the current graph, all levels kept
+  // the base (delta mode): the current graph's levels, all kept, built with
+  // 1024-source windows and read as 128-source sub-windows (nwin of them)
   int nwin = 0, level_cap = 0, base_T = 0, base_teams = 0;
   uint4* d_levels = nullptr;
   int nbw = 0;                        // base windows of 1024 sources
