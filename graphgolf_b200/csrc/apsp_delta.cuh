@@ -2,9 +2,10 @@
 //
 // A 2-opt swap changes four adjacency entries, and only a few thousand of
 // the N^2 distances.  The base build (apsp_base_kernel) evaluates the
-// current graph once with windows of 128 sources and keeps every level's
-// bitset rows S_k, each level's popcount and each window's completion level.
-// A candidate is then evaluated window by window from the base alone:
+// current graph once with windows of 1024 sources and keeps every level's
+// bitset rows S_k; base_counts_kernel and sub_levels_kernel derive each
+// level's popcount and the completion level of every 128-source sub-window.
+// A candidate is then evaluated sub-window by sub-window from the base alone:
 //
 //   S'_0 = S_0 (the identity), and for k >= 0
 //   S'_{k+1}[v] = S'_k[v] | OR_{u in N'(v)} S'_k[u]          (the recurrence of
