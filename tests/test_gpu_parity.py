@@ -125,7 +125,7 @@ def test_repeated_calls_identical(gpu):
 
 
 def test_large_properties(gpu):
-    """BASELINE-size graph: the GPU total equals the golden, and the symmetric
+    """The headline-size graph (N=65536, d=16): the GPU total equals the golden, and the symmetric
     g=16 variant runs 1/16 of the sources yet gives the same-size total."""
     for c in golden_cases():
         if c["nodes"] == 65536:
