@@ -691,9 +691,16 @@ __global__ void __launch_bounds__(kThreads, 1) endpoint_sweep_kernel(const Endpo
       const int nb = lane < d ? __ldg(e.adj + (long long)v * d + lane) : 0;
       const unsigned own = lane < nw ? __ldcg(A + (size_t)v * nw + lane) : 0u;
       unsigned acc = own;
-      for (int j = 0; j < d; ++j) {
-        const int u = __shfl_sync(0xffffffffu, nb, j);
-        if (lane < nw) acc |= __ldcg(A + (size_t)u * nw + lane);
+      for (int j0 = 0; j0 < d; j0 += 8) {   // eight neighbour words in flight a lane
+        unsigned x[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const int j = j0 + q;
+          const int u = __shfl_sync(0xffffffffu, nb, j & 31);
+          x[q] = (j < d && lane < nw) ? __ldcg(A + (size_t)u * nw + lane) : 0u;
+        }
+#pragma unroll
+        for (int q = 0; q < 8; ++q) acc |= x[q];
       }
       for (int f = __ldcg(e.head + v); f >= 0; f = __ldcg(e.next + f)) {   // the same list in every lane
         const int c = f >> 2, q = f & 3;
