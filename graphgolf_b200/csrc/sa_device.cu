@@ -1125,7 +1125,10 @@ int create(ggb_sa* a, int nodes, int degree, const int* edges, int K, int G, int
     if ((rc = check_sticky(a))) return rc;
     size_t free_b = 0, total_b = 0;
     SCUDA(cudaMemGetInfo(&free_b, &total_b));
-    const double base_bytes = (double)((nodes + 1023) / 1024) * 8 * (c.diam + 1) * nodes * 16.0;
+    // the kept levels plus the build's two row buffers per team (at most one team per SM or per window)
+    const int nbw = (nodes + 1023) / 1024;
+    const double base_bytes = (double)nbw * ggb::kBaseR * (c.diam + 1) * nodes * 16.0 +
+                              (double)std::min(a->sms, nbw) * 2 * nodes * ggb::kBaseR * 16.0;
     if (c.done && !c.disconnected && c.diam < nodes && base_bytes <= 0.25 * (double)free_b) {
       a->level_cap = std::max(2, c.diam);
       if ((rc = alloc_base(a))) return rc;
