@@ -160,6 +160,141 @@ def survey_formula_bytes(nodes: int, degree: int, levels: int, window_bits: int)
     return levels * (nodes * degree * 4 + nodes * degree * row + 2 * nodes * row)
 
 
+def _profile(workload: str) -> dict:
+    """Per-launch DRAM and L2 bytes of the committed ncu captures of this
+    workload (profiles/apsp_<workload>_traffic.json), or {}."""
+    tp = ROOT / "profiles" / f"apsp_{workload}_traffic.json"
+    return json.loads(tp.read_text()) if tp.exists() else {}
+
+
+def l2_gather_roof(lib, n: int, d: int, window_bits: int):
+    """The measured roof of a dense sweep: ggb_probe_l2_gather's random-row OR
+    sweeps with the kernel's own access width at the same N, d and W, in GB/s
+    of the sweep's algorithmic bytes (None if the probe fails)."""
+    g = C.c_double(0)
+    return g.value if lib.ggb_probe_l2_gather(n, d, window_bits, 20, C.byref(g)) == 0 and g.value > 0 else None
+
+
+def roofline(kernel: str, alg: float, ms: float, l2_roof, hbm_peak: float, hbm_kind: str, traffic, lts,
+             lts_pct=None) -> dict:
+    """Roofline of one kernel launch.  The sweeps' working set is L2-resident
+    by design, so the bound is the L2 random-row gather rate measured live by
+    the probe; the physical DRAM traffic (from the committed ncu capture) is
+    reported against the measured HBM copy bandwidth beside it."""
+    achieved = alg / (ms / 1e3) / 1e9
+    out = {"bound": "l2", "achieved": achieved, "peak": l2_roof, "unit": "GB/s",
+           "frac": (achieved / l2_roof) if l2_roof else None, "traffic": traffic, "kernel": kernel,
+           "ms_per_launch": ms, "algorithmic_bytes_per_launch": alg,
+           "peak_source": "ggb_probe_l2_gather: random-row OR sweeps with the kernel's own 32-byte accesses "
+                          "at the same N, d and window, measured in this run (algorithmic bytes per second)",
+           "hbm_peak_gbs": hbm_peak,
+           "hbm_peak_source": "measured hbm_gbs (MEASURED_PEAKS.json)" if hbm_kind == "measured"
+           else "fallback 6650 GB/s"}
+    if traffic:
+        out["dram_gbs"] = traffic / (ms / 1e3) / 1e9
+        out["dram_frac"] = out["dram_gbs"] / hbm_peak
+    if lts:
+        out["lts_bytes_per_launch"] = lts
+        out["lts_gbs"] = lts / (ms / 1e3) / 1e9
+    if lts_pct is not None:
+        out["lts_throughput_pct"] = lts_pct
+    out["note"] = ("traffic = DRAM bytes per launch from the committed ncu capture under profiles/; "
+                   "achieved counts every gather of every dense sweep, including the lanes the last-level "
+                   "skip leaves out")
+    return out
+
+
+def width_sweep(lib, one, n: int, d: int, groups: int, args) -> dict:
+    """The headline graph at forced source-window widths of 64, 128, 256 and
+    512 bits (the reference's one-word chunk and its vector widths): evals/s
+    over CUDA events on the launching stream (L2 flushed before each step),
+    the persistent kernel's time, its algorithmic GB/s, and DRAM / L2 GB/s
+    from the committed ncu launch list of the same widths."""
+    import graphgolf_b200 as gg
+    import torch
+    prof = _profile(f"{args.workload}_widths")
+    out = {"steps": 3, "rows": []}
+    for bits in (64, 128, 256, 512):
+        gg.set_tuning(bits, 0)
+        one()
+        lib.ggb_set_timing(1)
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(3)]
+        kms = []
+        for e in evs:
+            r = one(e)
+            mb, mp = C.c_double(0), C.c_double(0)
+            if lib.ggb_kernel_times(C.byref(mb), C.byref(mp)) == 0:
+                kms.append(mp.value)
+        lib.ggb_set_timing(0)
+        torch.cuda.synchronize()
+        ms = statistics.mean(a.elapsed_time(b) for a, b in evs)
+        km = statistics.mean(kms) if kms else ms
+        alg = sweep_bytes(n, d, r.dense_levels, r.window_bits)
+        row = {"window_bits": r.window_bits, "windows": r.windows, "dense_levels": r.dense_levels,
+               "evals_per_s": 1e3 / ms, "ms_per_eval": ms, "kernel_ms": km,
+               "algorithmic_gbs": alg / (km / 1e3) / 1e9, "total": r.total, "diameter": r.diameter}
+        pk = prof.get(str(bits), {})
+        if pk.get("dram_bytes_per_launch"):
+            row["dram_gbs"] = pk["dram_bytes_per_launch"] / (km / 1e3) / 1e9
+        if pk.get("lts_bytes_per_launch"):
+            row["l2_gbs"] = pk["lts_bytes_per_launch"] / (km / 1e3) / 1e9
+        out["rows"].append(row)
+    out["same_answer"] = len({(x["diameter"], x["total"]) for x in out["rows"]}) == 1
+    out["traffic_source"] = ("profiles/apsp_n65536d16_widths_traffic.json (ncu launch list, one pass)"
+                             if prof else None)
+    return out
+
+
+def g16_block(lib, hbm_peak: float, hbm_kind: str) -> dict:
+    """The symmetric variant of the headline graph: 16 rotation groups
+    (v <-> v + N/16), so only 4096 of the 65536 sources run; evals/s with the
+    adjacency resident (L2 flushed before each step, CUDA events on the
+    launching stream) and the kernel's roofline."""
+    import numpy as np
+    import torch
+    from graphgolf_b200 import _native, graphs
+    wl = WORKLOADS["n65536d16g16"]
+    n, d, grp = wl["nodes"], wl["degree"], wl["groups"]
+    g = graphs.symmetric_regular(n, d, grp, wl["seed"])
+    adj_dev = torch.from_numpy(np.ascontiguousarray(g.adj)).cuda()
+    stream = torch.cuda.Stream()
+    sptr = C.c_void_p(stream.cuda_stream)
+    flush = torch.empty(512 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+    res = _native.ggb_result()
+    lib.ggb_set_timing(1)
+    evs, kms = [], []
+    for k in range(13):
+        e = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+        with torch.cuda.stream(stream):
+            flush.fill_(1)
+            e[0].record(stream)
+            if lib.ggb_launch_general_device(n, n // grp, grp, d, adj_dev.data_ptr(), 0, sptr):
+                raise RuntimeError(_native.last_error())
+            e[1].record(stream)
+        if lib.ggb_collect(sptr, C.byref(res)):
+            raise RuntimeError(_native.last_error())
+        mb, mp = C.c_double(0), C.c_double(0)
+        if k >= 3:
+            evs.append(e)
+            if lib.ggb_kernel_times(C.byref(mb), C.byref(mp)) == 0:
+                kms.append(mp.value)
+    lib.ggb_set_timing(0)
+    torch.cuda.synchronize()
+    ms = statistics.mean(a.elapsed_time(b) for a, b in evs)
+    km = statistics.mean(kms) if kms else ms
+    r = _native.ggb_result()
+    alg = sweep_bytes(n, d, res.dense_levels, res.window_bits)
+    kp = _profile("n65536d16g16").get("apsp_persistent_kernel", {})
+    roof = roofline(f"apsp_persistent_kernel<{res.window_bits // 128}>", alg, km,
+                    l2_gather_roof(lib, n, d, res.window_bits), hbm_peak, hbm_kind,
+                    kp.get("dram_bytes_per_launch"), kp.get("lts_bytes_per_launch"))
+    del r
+    return {"workload": "n65536d16g16: rotationally symmetric 16-regular graph, N=65536, g=16 (4096 sources)",
+            "evals_per_s": 1e3 / ms, "ms_per_eval": ms, "kernel_ms": km, "window_bits": res.window_bits,
+            "windows": res.windows, "dense_levels": res.dense_levels, "diameter": res.diameter,
+            "total": res.total, "steps": len(evs), "roofline": roof}
+
+
 def cpu_baseline(adj, budget_s: float = 12.0):
     """The reference OpenMP evaluator on this host, bounded to ~budget_s."""
     import oracle
@@ -193,9 +328,23 @@ def cpu_baseline(adj, budget_s: float = 12.0):
             "sample": f"rank 0 of {procs} (1/{procs} of the source chunks) in {el:.2f} s"}
 
 
+def common_config(args, wl: dict) -> dict:
+    """The `config` both arms print: the workload by name and size, the L2
+    policy and the parallelism (identical strings in both arms)."""
+    return {"workload": args.workload, "nodes": wl["nodes"], "degree": wl["degree"], "groups": wl["groups"],
+            "seed": wl["seed"],
+            "l2_policy": "GPU arm: 512 MiB flush write before every timed step, outside the events; "
+                         "CPU reference arm: none (no cache to flush between full evaluations)",
+            "parallelism": f"independent graph per rank x{args.gpus}"}
+
+
 def run_reference_arm(args, wl):
-    import numpy as np  # noqa: F401
+    """The reference's own OpenMP evaluator (general/evaluation.c, compiled
+    from its sources into oracle/_ref) on the same graph.  The graph is drawn
+    by oracle.graphgen, a pure-Python copy of the package's generator, so this
+    process loads none of the package's libraries."""
     import oracle
+    from oracle import graphgen
     rank = _env_int("RANK", 0)
     if rank != 0:
         return 0
@@ -203,28 +352,34 @@ def run_reference_arm(args, wl):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built from the reference "
                           "sources (reference tree absent at build time)"}))
         return 0
-    g = _graph(wl, 0)
+    n, d, grp = wl["nodes"], wl["degree"], wl["groups"]
+    if grp > 1:
+        edges = graphgen.symmetric_regular_edges(n, d, grp, wl["seed"])
+    else:
+        edges = graphgen.random_regular_edges(n, d, wl["seed"])
+    adj = graphgen.create_adj(n, d, edges)
     threads = os.cpu_count() or 1
     os.environ["OMP_NUM_THREADS"] = str(threads)
     t0 = time.perf_counter()
-    oracle.ref_general(g.adj, procs=64, rank=0, groups=wl["groups"])
+    oracle.ref_general(adj, procs=64, rank=0, groups=grp)
     est_full = (time.perf_counter() - t0) * 64
     # each step is one full evaluation unless that would take the whole run past ~3 minutes
     procs = 1
     while procs < 64 and est_full / procs * (args.steps + args.warmup) > 150:
         procs *= 2
     for _ in range(args.warmup):
-        oracle.ref_general(g.adj, procs=procs, rank=0, groups=wl["groups"])
+        oracle.ref_general(adj, procs=procs, rank=0, groups=grp)
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        oracle.ref_general(g.adj, procs=procs, rank=0, groups=wl["groups"])
+        ok, diam, aspl = oracle.ref_general(adj, procs=procs, rank=0, groups=grp)
     el = time.perf_counter() - t0
     value = args.steps / procs / el
     sample = "one full evaluation per step" if procs == 1 else f"rank 0 of {procs} source-chunk shares per step"
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic (seeded random regular graph)",
-            "config": {"workload": args.workload, **wl}, "impl": "reference",
+            "config": common_config(args, wl), "impl": "reference",
+            "answer": {"diameter": diam, "aspl": aspl} if procs == 1 else None,
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
                              "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -243,6 +398,8 @@ def main() -> int:
     ap.add_argument("--no-ref-gpu", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the mixed-batch measurement")
     ap.add_argument("--no-sa", action="store_true", help="skip the annealing race")
+    ap.add_argument("--no-widths", action="store_true",
+                    help="skip the window-width sweep (64..512 bits) and the g=16 symmetric graph")
     ap.add_argument("--sa-plain-steps", type=int, default=30000, help="plain annealing steps that set the target")
     ap.add_argument("--flush-mib", type=int, default=512, help="L2 flush buffer written before every step")
     ap.add_argument("--window-bits", type=int, default=0, help="force the source-window width (0 = automatic)")
@@ -360,37 +517,22 @@ def main() -> int:
     ball_ms = statistics.mean(kt_ball) if kt_ball else 0.0
     alg = sweep_bytes(n, d, first.dense_levels, first.window_bits)
     achieved = alg / (pers_ms / 1e3) / 1e9
-    l2_peak = C.c_double(0)
-    l2_ok = lib.ggb_probe_l2_gather(n, d, first.window_bits, 20, C.byref(l2_peak)) == 0
-    prof = {}
-    tp = ROOT / "profiles" / f"apsp_{args.workload}_traffic.json"
-    if tp.exists():
-        prof = json.loads(tp.read_text())
-    traffic = prof.get("apsp_persistent_kernel", {}).get("dram_bytes_per_launch")
-    lts = prof.get("apsp_persistent_kernel", {}).get("lts_bytes_per_launch")
+    l2_roof = l2_gather_roof(lib, n, d, first.window_bits)
+    prof = _profile(args.workload)
+    kp = prof.get("apsp_persistent_kernel", {})
+    traffic = kp.get("dram_bytes_per_launch")
+    lts = kp.get("lts_bytes_per_launch")
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": mean_ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u64",
             "data": "synthetic (seeded random regular graph, per-pair-retry pairing model)",
-            "config": {"workload": args.workload, "nodes": n, "degree": d, "groups": groups,
-                       "sources": bn, "window_bits": first.window_bits, "windows": first.windows,
-                       "levels": first.levels, "dense_levels": first.dense_levels,
-                       "diameter": first.diameter, "total": first.total,
-                       "l2_policy": f"{max(args.flush_mib, 200)} MiB flush write before every timed step (outside the events)",
-                       "parallelism": f"independent graph per rank x{world}"},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic,
-                         "kernel": f"apsp_persistent_kernel<{first.window_bits // 128}>",
-                         "ms_per_launch": pers_ms,
-                         "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured"
-                         else "fallback 6650 GB/s",
-                         "algorithmic_bytes_per_launch": alg,
-                         "l2_gather_peak_gbs": l2_peak.value if l2_ok else None,
-                         "frac_of_l2_gather_peak": (achieved / l2_peak.value) if l2_ok and l2_peak.value else None,
-                         "lts_bytes_per_launch": lts,
-                         "note": "the window working set is L2-resident by design; traffic = DRAM bytes per "
-                                 "launch from the committed ncu capture under profiles/"},
+            "config": common_config(args, wl),
+            "run": {"sources": bn, "window_bits": first.window_bits, "windows": first.windows,
+                    "levels": first.levels, "dense_levels": first.dense_levels,
+                    "diameter": first.diameter, "total": first.total, "aspl": first.aspl},
+            "roofline": roofline(f"apsp_persistent_kernel<{first.window_bits // 128}>", alg, pers_ms, l2_roof,
+                                 peak, peak_kind, traffic, lts, kp.get("lts_throughput_pct")),
             "ball_prepass": {"ms_per_launch": ball_ms,
                              "algorithmic_bytes_per_launch": ball_bytes(n, d, first.windows, first.window_bits)
                              if ball_ms else 0,
@@ -401,12 +543,17 @@ def main() -> int:
             "gpu_launches": int(launches),
             "clocks": clk.summary()}
 
+    if rank == 0 and world == 1 and not args.no_widths and groups == 1:
+        line["widths"] = width_sweep(lib, one, n, d, groups, args)
+        gg.set_tuning(args.window_bits, 0)
+    if rank == 0 and world == 1 and not args.no_widths and args.workload == "n65536d16":
+        line["g16"] = g16_block(lib, peak, peak_kind)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(host_adj)
     if rank == 0 and world == 1 and not args.no_ref_gpu and groups == 1:
         line["reference_cuda"] = reference_cuda(host_adj, first)
     if rank == 0 and world == 1 and not args.no_batch:
-        line["batch"] = batch_bench(peak, lib)
+        line["batch"] = batch_bench(peak, peak_kind, lib)
     if rank == 0 and world == 1 and not args.no_sa:
         line["sa"] = sa_bench(args.sa_plain_steps)
     if rank == 0:
@@ -417,7 +564,7 @@ def main() -> int:
     return 0
 
 
-def batch_bench(peak: float, lib) -> dict:
+def batch_bench(peak: float, peak_kind: str, lib) -> dict:
     """The mixed batch: a 4096-vertex 12-regular base graph and 256 seeded
     2-opt candidates of 12-regular graphs with 512..16384 vertices, all in one
     cooperative launch replayed from a CUDA graph, plan autotuned.  value =
@@ -448,52 +595,49 @@ def batch_bench(peak: float, lib) -> dict:
     e2e_ms = (time.perf_counter() - t0) / 5 * 1e3
     kms = statistics.median(ms)
     alg = sum(sweep_bytes(x.nodes, 12, r.dense_levels, r.window_bits) for x, r in zip(w, res))
-    achieved = alg / (kms / 1e3) / 1e9
-    l2 = C.c_double(0)
-    l2_ok = lib.ggb_probe_l2_gather(16384, 12, bits, 10, C.byref(l2)) == 0
+    l2 = l2_gather_roof(lib, 16384, 12, bits)
     b.close()
+    roof = roofline(f"apsp_batch_kernel<{bits // 128}>", alg, kms, l2, peak, peak_kind, None, None)
+    roof["peak_source"] += " (probed at N=16384, d=12: the largest graphs of the batch)"
     return {"workload": "4096-vertex base + 256 single-swap candidates, d=12, N log-uniform 512..16384",
             "graphs": len(w), "plan": {"window_bits": bits, "team_ctas": team, "autotune_s": tune_s},
             "value": len(w) / (kms / 1e3), "unit": "graphs/s", "ms_per_batch": kms,
             "e2e": {"value": len(w) / (e2e_ms / 1e3), "unit": "graphs/s", "ms_per_batch": e2e_ms,
                     "h2d_bytes_per_step": int(sum(a.nbytes for a in adjs)), "d2h_bytes_per_step": 48 * len(w)},
-            "roofline": {"bound": "hbm", "kernel": f"apsp_batch_kernel<{bits // 128}>", "achieved": achieved,
-                         "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "algorithmic_bytes_per_launch": alg,
-                         "l2_gather_peak_gbs": l2.value if l2_ok else None,
-                         "frac_of_l2_gather_peak": achieved / l2.value if l2_ok and l2.value else None},
+            "roofline": roof,
             "checked": "4 graphs bit-identical to the single-graph evaluator"}
 
 
-def sa_bench(plain_steps: int) -> dict:
-    """Annealing race on a seeded random 12-regular graph, N=16384 (hill
-    climbing, the reference's -H rule).  Plain device annealing (one random
-    2-opt candidate per step, evaluated in full: the reference's step) runs
-    plain_steps steps; its final exact distance total is the target.  The
-    batched+learned annealer (4096 proposals per step ranked by the trained
-    network, the best 256 evaluated exactly against the base, the disjoint
-    exact improvers composed and evaluated in full) and the batched one
-    without the network then run until they reach the same exact total.
-    Wall seconds on the host clock around the runs (each run synchronises)."""
+def _race(g, plain_steps: int, schedule, rows) -> dict:
+    """Plain device annealing (one random 2-opt candidate per step, evaluated
+    in full: the reference's step) runs plain_steps steps under `schedule`;
+    its best exact (diameter, distance total) is the target.  Each annealer of
+    `rows` (name, candidates K, proposals G) then runs under the same schedule
+    until its current graph reaches the target (at most 90 s).  Wall seconds
+    on the host clock around runs that synchronise; every final graph is
+    re-evaluated in full."""
     import graphgolf_b200 as gg
     from graphgolf_b200 import graphs
-    g = graphs.random_regular(16384, 12, 2)
-    out = {"workload": "random 12-regular, N=16384, hill climbing, seed 2", "plain_steps": plain_steps}
-    an = gg.Annealer(g, 1, 1, 0, seed=1)
+
+    def prep(a):
+        if schedule is not None:
+            a.schedule(*schedule, hill_climbing=False)
+        return a
+
+    an = prep(gg.Annealer(g, 1, 1, 0, seed=1))
     st0 = an.run(0)
     t0 = time.perf_counter()
     st = an.run(plain_steps)
     t_plain = time.perf_counter() - t0
     an.close()
-    out["start_aspl"] = st0.cur_aspl
-    out["target_aspl"] = st.cur_aspl
-    out["target_total"] = st.cur_total
-    out["plain"] = {"wall_s": t_plain, "steps": st.step, "accepts": st.accepts, "evals": st.evals}
-    for name, K, G in (("learned", 256, 4096), ("batched", 256, 256)):
-        a = gg.Annealer(g, K, G, K, seed=1)
+    out = {"start_aspl": st0.cur_aspl, "target_diameter": st.best_diam, "target_total": st.best_total,
+           "target_aspl": st.best_aspl,
+           "plain": {"wall_s": t_plain, "steps": st.step, "accepts": st.accepts, "evals": st.evals}}
+    for name, K, G in rows:
+        a = prep(gg.Annealer(g, K, G, K, seed=1))
         if G > K:
             a.predicted(0, 1)
-        a.target(st.cur_diam, st.cur_total)
+        a.target(st.best_diam, st.best_total)
         s = a.run(0)
         t0 = time.perf_counter()
         while not s.done and time.perf_counter() - t0 < 90:
@@ -501,12 +645,71 @@ def sa_bench(plain_steps: int) -> dict:
         el = time.perf_counter() - t0
         edges = a.edges()
         a.close()
-        adj = graphs.create_adj(g.nodes, g.degree, edges)
-        r = gg.evaluate(adj)
+        r = gg.evaluate(graphs.create_adj(g.nodes, g.degree, edges))
         out[name] = {"wall_s": el, "reached": bool(s.done), "steps": s.step, "accepts": s.accepts,
                      "moved_swaps": s.moved_swaps, "evals": s.evals, "final_aspl": s.cur_aspl,
                      "final_checked": (r.diameter, r.total) == (s.cur_diam, s.cur_total),
                      "candidates": K, "proposals": G, "speedup_vs_plain": t_plain / el if s.done else None}
+    return out
+
+
+def reference_sa_time(g, steps: int, temp_max: float, temp_min: float):
+    """The reference's own annealer (general/{main,sa,common,evaluation}.c with
+    OpenMP, oracle/_ref/gg_openmp) on the same graph, all host cores: its
+    `Elapse time` line (general/main.c:479) over a bounded sample of steps."""
+    import re
+    import subprocess
+    import tempfile
+    import oracle
+    from graphgolf_b200 import graphs
+    prog = oracle.REF_DIR / "gg_openmp"
+    if not prog.exists():
+        return None
+    threads = os.cpu_count() or 1
+    with tempfile.TemporaryDirectory() as td:
+        f = os.path.join(td, "in.edges")
+        graphs.write_general(f, g)
+        env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+        p = subprocess.run([str(prog), "-f", f, "-M", "-s", "1", "-n", str(steps), "-w", str(temp_max),
+                            "-c", str(temp_min)], cwd=td, capture_output=True, text=True, env=env, timeout=600)
+    m = re.search(r"Steps: (\d+),?\s+Elapse time: ([0-9.]+) sec\. \(APSP: ([0-9.]+)", p.stdout)
+    if p.returncode != 0 or not m:
+        return {"error": f"rc {p.returncode}", "tail": p.stdout[-300:]}
+    st, el, apsp = int(m.group(1)), float(m.group(2)), float(m.group(3))
+    return {"steps": st, "elapse_s": el, "apsp_s": apsp, "s_per_step": el / max(st, 1), "cores": threads,
+            "what": "reference gg_openmp (OpenMP evaluator, one MPI rank) 'Elapse time' over a bounded sample"}
+
+
+def sa_bench(plain_steps: int) -> dict:
+    """The learned-filter configuration on a seeded random 12-regular graph,
+    N=16384: simulated annealing with the reference's Metropolis rule
+    (general/sa.c:371-411) and geometric cooling from temperature 100 to
+    0.0001 over the plain run's steps (general/main.c:441, sa.c:508).  Plain
+    device annealing sets the target; the learned annealer (4096 proposals per
+    step ranked by the online-trained network, the best 64 evaluated exactly
+    against the kept base, disjoint exact improvers composed) and the same
+    batched annealer without the network (64 random proposals) race to it.
+    The network's own gain is batched / learned.  A second race uses hill
+    climbing with the best 256 (the reference's -H rule).  The reference's own
+    CPU annealer is timed on the same graph over a bounded sample of steps."""
+    from graphgolf_b200 import graphs
+    g = graphs.random_regular(16384, 12, 2)
+    t_max, t_min = 100.0, 0.0001
+    cooling = (t_min / t_max) ** (1.0 / plain_steps)
+    out = {"workload": "random 12-regular, N=16384, seed 2", "plain_steps": plain_steps,
+           "schedule": {"temp_max": t_max, "temp_min": t_min, "cooling_per_step": cooling}}
+    sa = _race(g, plain_steps, (t_max, cooling), (("learned", 64, 4096), ("batched", 64, 64)))
+    if sa["learned"]["reached"] and sa["batched"]["reached"]:
+        sa["network_gain"] = sa["batched"]["wall_s"] / sa["learned"]["wall_s"]
+    out["annealing"] = sa
+    hill = _race(g, plain_steps, None, (("learned", 256, 4096), ("batched", 256, 256)))
+    if hill["learned"]["reached"] and hill["batched"]["reached"]:
+        hill["network_gain"] = hill["batched"]["wall_s"] / hill["learned"]["wall_s"]
+    out["hill_climbing"] = hill
+    ref = reference_sa_time(g, 100, t_max, t_min)
+    if ref and "s_per_step" in ref:
+        ref["extrapolated_plain_steps_s"] = ref["s_per_step"] * plain_steps
+    out["reference_cpu_sa"] = ref
     return out
 
 

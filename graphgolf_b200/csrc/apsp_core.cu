@@ -111,6 +111,7 @@ struct State {
   ApspCtrl* h_ctrl = nullptr;
   // tuning
   int force_R = 0;
+  int force_W = 0;            // forced sources per window below 128 (64), else 0
   int force_ctas = 0;
   long long timeout_ns = 2000000000LL;
   int phantom = 0;
@@ -128,7 +129,7 @@ struct State {
   int occ[8] = {0, 0, 0, 0, 0, 0, 0, 0};   // co-resident CTAs per SM, per R index
   int smem_optin = 0;
   // last launch bookkeeping (for ggb_collect)
-  int last_N = 0, last_R = 0;
+  int last_N = 0, last_R = 0, last_W = 0;
   bool pending = false;
   bool last_grid = false;
 };
@@ -303,12 +304,12 @@ int launch_apsp(const int* d_adj, int N, int d, int n_src1, int split, int ac, i
   // reads per vertex, one HBM write of every window's S_3 rows) is below what
   // it saves (per window: the two-hop seeding and one dense sweep).
   const bool vec4 = (d % 4 == 0 && ((uintptr_t)d_adj % 16) == 0);
-  const int W = 128 * R;
+  const int W = (R == 1 && g.force_W > 0) ? g.force_W : 128 * R;
   const int nwin1 = n_src1 > 0 ? (n_src1 + W - 1) / W : 0;
   const int n_local = nwin1 > rank ? (nwin1 - rank + procs - 1) / procs : 0;
   const size_t ball_cells = (size_t)n_local * N * R;
   const size_t ball_smem = ggb::ball_smem_bytes(n_src1, d, std::max(n_local, 1));
-  bool use_ball = g.ball_mode != 0 && ac == 0 && n_local >= 1 && n_local <= ggb::kBallMaxWindows && d >= 1 &&
+  bool use_ball = g.ball_mode != 0 && ac == 0 && W == 128 * R && n_local >= 1 && n_local <= ggb::kBallMaxWindows && d >= 1 &&
                   d <= ggb::kBallMaxDegree && ball_smem <= (size_t)(g.smem_optin - 4096) &&
                   ball_cells * 16 <= ((size_t)8 << 30);
   if (use_ball && g.ball_mode < 0) {
@@ -353,6 +354,7 @@ int launch_apsp(const int* d_adj, int N, int d, int n_src1, int split, int ac, i
   a.vec4 = vec4 ? 1 : 0;
   a.ball = use_ball ? g.d_ball : nullptr;
   a.ball_cnt = use_ball ? g.d_ball_cnt : nullptr;
+  a.win_bits = W < 128 * R ? W : 0;
   CUDA_TRY(cudaMemsetAsync(g.d_ctrl, 0, sizeof(ApspCtrl), st));
   if (g.timing) CUDA_TRY(cudaEventRecord(g.ev[0], st));
   if (use_ball) {
@@ -391,6 +393,7 @@ int launch_apsp(const int* d_adj, int N, int d, int n_src1, int split, int ac, i
   g.ev_ball = use_ball;
   g.last_N = N;
   g.last_R = R;
+  g.last_W = W;
   g.pending = true;
   return GGB_OK;
 }
@@ -416,7 +419,7 @@ int read_ctrl(cudaStream_t st, ggb_partial* p) {
   p->levels = c.levels;
   p->dense_levels = c.dense_levels;
   p->windows = c.windows;
-  p->window_bits = 128 * g.last_R;
+  p->window_bits = g.last_W;
   g.trace_len = c.trace_len;
   return GGB_OK;
 }
@@ -534,9 +537,10 @@ void ggb_finalize(void) {
   cudaFreeHost(g.h_rh);
   cudaFreeHost(g.h_ctrl);
   if (g.stream) cudaStreamDestroy(g.stream);
-  const int fr = g.force_R, fc = g.force_ctas, bm = g.ball_mode;
+  const int fr = g.force_R, fw = g.force_W, fc = g.force_ctas, bm = g.ball_mode;
   g = State();
   g.force_R = fr;
+  g.force_W = fw;
   g.force_ctas = fc;
   g.ball_mode = bm;
 }
@@ -544,11 +548,13 @@ void ggb_finalize(void) {
 int ggb_set_tuning(int window_bits, int ctas) {
   std::lock_guard<std::mutex> lk(g_mu);
   if (window_bits < 0 || ctas < 0) return fail(GGB_EINVAL, "negative tuning value");
-  if (window_bits) {
+  if (window_bits && window_bits != 64) {
     if (window_bits % 128 || r_index(window_bits / 128) < 0)
-      return fail(GGB_EINVAL, "window_bits must be 128 * (1,2,4,...,64)");
+      return fail(GGB_EINVAL, "window_bits must be 64 or 128 * (1,2,4,...,64)");
   }
-  g.force_R = window_bits / 128;
+  // 64-source windows run on one-uint4 rows (R = 1) with the upper half unused
+  g.force_R = window_bits == 64 ? 1 : window_bits / 128;
+  g.force_W = window_bits == 64 ? 64 : 0;
   g.force_ctas = ctas;
   return GGB_OK;
 }

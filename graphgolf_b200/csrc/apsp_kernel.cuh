@@ -100,6 +100,10 @@ struct ApspArgs {
   long long* level_counts;
   int* win_levels;
   int level_cap;
+  // Sources per window when narrower than the rows: 64 runs 64-source windows
+  // (the reference's one-word chunk, general/evaluation.cu:27-44) on rows of
+  // one uint4 whose upper 64 bits stay zero.  0: W = 128 * R.
+  int win_bits = 0;
 };
 
 __device__ __forceinline__ unsigned long long globaltimer_ns() {
@@ -817,7 +821,7 @@ __device__ __forceinline__ bool eval_windows(const ApspArgs& a, int cta, int nct
   constexpr int LPR = R >= 32 ? 32 : R;
   constexpr int VPW = 32 / LPR;
   constexpr int UPL = R / LPR;
-  constexpr int W = 128 * R;
+  const int W = (a.win_bits > 0 && a.win_bits < 128 * R) ? a.win_bits : 128 * R;
   constexpr int U = UPL >= 2 ? 8 : 16;  // neighbour rows in flight per thread
   constexpr int SROW = 4 * R;          // 32-bit words per row in shared memory
   unsigned long long (*const s_red)[4] = sm.red;
@@ -854,7 +858,12 @@ __device__ __forceinline__ bool eval_windows(const ApspArgs& a, int cta, int nct
     const bool use_ball = phase == 1 && a.ball != nullptr;
     const int* __restrict__ adjp = (phase == 2 && a.adj2) ? a.adj2 : a.adj;
     int local = 0;
-    for (int t = a.win_first; t < nwin && !disconnected; t += a.win_stride, ++local) {
+    // The added-centre windows of rank r start at (r - based_nodes % procs)
+    // mod procs, as the reference's do (general/evaluation.c:209-212).
+    const int t_first = phase == 1 ? a.win_first
+                                   : ((a.win_first - a.n_src1 % a.win_stride) % a.win_stride + a.win_stride) %
+                                         a.win_stride;
+    for (int t = t_first; t < nwin && !disconnected; t += a.win_stride, ++local) {
       const int first = t * W;
       const int l = min(W, nsrc - first);
       const long long lo_rows = a.split, hi_rows = (long long)N - a.split;

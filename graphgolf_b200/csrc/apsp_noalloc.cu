@@ -14,7 +14,9 @@
 // must never hand it to a kernel.  The first call on a device, with that
 // device current, asks the runtime for the array's device address
 // (cudaGetSymbolAddress) and keeps it for later calls on that device; make
-// that first call before any stream capture.  All calls share the one array
+// that first call before any stream capture.  Every call waits for its own
+// result: it copies the result block to the host and synchronises `stream`.
+// All calls share the one array
 // and it keeps the previous call's contents: the control block is cleared at
 // the start of every call (the bitset rows are always fully written before
 // they are read).  Calls that overlap on the GPU -- from two host threads, or
@@ -22,8 +24,11 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cstdint>
+#include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <mutex>
 
 #include "../../include/graphgolf_b200.h"
@@ -34,6 +39,7 @@ namespace {
 constexpr size_t kNoAllocScratchBytes = (size_t)16 << 20;   // 16 MiB
 constexpr size_t kCtrlBytes = 256;                          // control block, padded
 constexpr int kMaxDevices = 64;
+static_assert(sizeof(ggb::ApspCtrl) <= kCtrlBytes, "the control block must fit its padded slot");
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
@@ -45,9 +51,16 @@ struct DeviceSlot {
 DeviceSlot g_slots[kMaxDevices];
 std::mutex g_mu;
 char g_err[256] = "";
+// Bound on every grid-barrier wait, as for the other entry points:
+// GGB_BARRIER_TIMEOUT_NS when set, else 2 s.  Read at the first call.
+long long g_timeout_ns = 0;
 
-int fail(int code, const char* msg) {
-  snprintf(g_err, sizeof g_err, "%s", msg);
+int fail(int code, const char* fmt, ...) __attribute__((format(printf, 2, 3)));
+int fail(int code, const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof g_err, fmt, ap);
+  va_end(ap);
   return code;
 }
 
@@ -86,7 +99,12 @@ int log2i(int R) {
 // Once per device, with that device current: resolve the scratch array's
 // device address and the kernels' occupancy.  Allocates nothing.
 int setup_device(int dev, DeviceSlot** out) {
-  if (dev < 0 || dev >= kMaxDevices) return fail(GGB_EINVAL, "device index out of range");
+  if (dev < 0 || dev >= kMaxDevices) return fail(GGB_EINVAL, "device index %d out of range", dev);
+  if (g_timeout_ns <= 0) {
+    const char* env = getenv("GGB_BARRIER_TIMEOUT_NS");
+    const long long t = env ? atoll(env) : 0;
+    g_timeout_ns = t > 0 ? t : 2000000000LL;
+  }
   DeviceSlot& s = g_slots[dev];
   if (!s.scratch) {
     void* p = nullptr;
@@ -127,6 +145,10 @@ extern "C" int ggb_eval_general_noalloc(int nodes, int based_nodes, int groups, 
   if (nodes <= 0 || based_nodes <= 0 || groups <= 0 || degree < 0 || added_centers < 0 ||
       (long long)based_nodes * groups + added_centers != nodes)
     return fail(GGB_EINVAL, "nodes must equal based_nodes*groups + added_centers, all sizes positive");
+  // The kernels index the adjacency with int offsets, as the reference's int
+  // adjacency does.
+  if ((long long)nodes * degree > INT_MAX)
+    return fail(GGB_EINVAL, "nodes*degree exceeds the int32 adjacency of the reference");
   // The two bitset matrices of a window need 2 * nodes * 16 bytes per 128
   // sources; the narrowest window (128 sources) must fit.
   const size_t avail = kNoAllocScratchBytes - kCtrlBytes;
@@ -158,7 +180,7 @@ extern "C" int ggb_eval_general_noalloc(int nodes, int based_nodes, int groups, 
   a.buf0 = bufs;
   a.buf1 = bufs + cells;
   a.ctrl = ctrl;
-  a.timeout_ns = 2000000000LL;
+  a.timeout_ns = g_timeout_ns;
   a.N = nodes;
   a.d = degree;
   a.n_src1 = based_nodes;
@@ -200,9 +222,13 @@ extern "C" int ggb_eval_general_noalloc(int nodes, int based_nodes, int groups, 
     cudaGetLastError();
     return fail(GGB_ECUDA, "reading the result block failed");
   }
-  if (c.error == ggb::kErrAdj) return fail(GGB_EADJ, "adjacency entry outside [0, nodes)");
-  if (c.error == ggb::kErrTimeout) return fail(GGB_ETIMEOUT, "a grid-barrier wait ran out");
-  if (c.error != 0 || !c.done) return fail(GGB_ECUDA, "the persistent kernel did not complete");
+  if (c.error == ggb::kErrAdj)
+    return fail(GGB_EADJ, "adjacency entry outside [0, nodes) (reported by CTA/vertex %d)", c.error_info);
+  if (c.error == ggb::kErrTimeout) return fail(GGB_ETIMEOUT, "a grid-barrier wait ran out (CTA %d)", c.error_info);
+  if (c.error == ggb::kErrDegree)
+    return fail(GGB_EINVAL, "degree of vertex %d outside [0, max_degree]", c.error_info);
+  if (c.error != 0) return fail(GGB_ECUDA, "device error code %d (at %d)", c.error, c.error_info);
+  if (!c.done) return fail(GGB_ECUDA, "the persistent kernel did not complete");
   ggb_partial p;
   p.diam = c.diam;
   p.disconnected = c.disconnected;

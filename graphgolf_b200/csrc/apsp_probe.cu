@@ -5,9 +5,10 @@
 // bandwidth but the rate at which the SMs can gather random rows of that size
 // from L2.  ggb_probe_l2_gather times exactly that access pattern -- every
 // vertex ORs its own row and the rows of its d random neighbours out of a
-// matrix of the same shape, one launch per sweep -- on buffers it allocates
-// itself, and reports gathered bytes per second.  bench.py uses it for the
-// roofline report.
+// matrix of the same shape, with the same 32-byte accesses, one launch per
+// sweep, at two CTAs per SM -- on buffers it allocates itself, and reports
+// the sweep's algorithmic bytes per second.  bench.py uses it as the roof of
+// its roofline report.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -15,47 +16,71 @@
 #include <vector>
 
 #include "../../include/graphgolf_b200.h"
+#include "apsp_kernel.cuh"
 
 namespace {
 
+// One sweep: every vertex ORs its own row and its d neighbours' rows and
+// writes the result, with the accesses the evaluator's dense sweeps issue:
+// 16-byte ld.global.cg for rows of one uint4 (windows of 64 or 128 sources),
+// otherwise 32-byte ld.global.cg.v8 accesses, LP lanes a row (a half-warp for
+// 512-byte rows, as in the 4096-source sweeps), U neighbour rows in flight.
 template <int R>
 __global__ void __launch_bounds__(512, 2) probe_gather_kernel(const uint4* __restrict__ src, uint4* __restrict__ dst,
                                                              const int* __restrict__ adj, int N, int d,
                                                              unsigned long long* sink) {
-  constexpr int LPR = R >= 32 ? 32 : R;
-  constexpr int VPW = 32 / LPR;
-  constexpr int UPL = R / LPR;
+  constexpr int PARTS = R >= 2 ? R / 2 : 1;          // accesses per row (32 bytes each, 16 for R = 1)
+  constexpr int LP = PARTS >= 32 ? 32 : PARTS;        // lanes per row
+  constexpr int PPL = PARTS / LP;                     // accesses per lane and row
+  constexpr int RPW = 32 / LP;                        // rows per warp step
+  constexpr int U = R >= 2 ? 4 : 8;                   // neighbour rows in flight
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int sub = lane / LPR, li = lane % LPR;
-  const long long slot = ((long long)blockIdx.x * 16 + warp) * VPW + sub;
-  const long long n_slots = (long long)gridDim.x * 16 * VPW;
+  const int sub = lane / LP, li = lane % LP;
+  const long long slot = ((long long)blockIdx.x * 16 + warp) * RPW + sub;
+  const long long n_slots = (long long)gridDim.x * 16 * RPW;
   unsigned c = 0;
   for (long long v = slot; v < N; v += n_slots) {
-    uint4 acc[UPL];
+    uint4 acc[PPL][2];
 #pragma unroll
-    for (int k = 0; k < UPL; ++k) acc[k] = __ldcg(src + v * R + li + k * LPR);
-    for (int j = 0; j < d; j += 8) {
-      uint4 x[8][UPL];
+    for (int p = 0; p < PPL; ++p) {
+      if constexpr (R >= 2) {
+        ggb::ld_cg2(src + v * R + 2 * (li + p * LP), acc[p]);
+      } else {
+        acc[p][0] = __ldcg(src + v);
+        acc[p][1] = make_uint4(0u, 0u, 0u, 0u);
+      }
+    }
+    for (int j = 0; j < d; j += U) {
+      uint4 x[U][PPL][2];
 #pragma unroll
-      for (int q = 0; q < 8; ++q) {
+      for (int q = 0; q < U; ++q) {
         const int u = j + q < d ? __ldg(adj + v * d + j + q) : (int)v;
 #pragma unroll
-        for (int k = 0; k < UPL; ++k) x[q][k] = __ldcg(src + (long long)u * R + li + k * LPR);
+        for (int p = 0; p < PPL; ++p) {
+          if constexpr (R >= 2) {
+            ggb::ld_cg2(src + (long long)u * R + 2 * (li + p * LP), x[q][p]);
+          } else {
+            x[q][p][0] = __ldcg(src + u);
+            x[q][p][1] = make_uint4(0u, 0u, 0u, 0u);
+          }
+        }
       }
 #pragma unroll
-      for (int q = 0; q < 8; ++q)
+      for (int q = 0; q < U; ++q)
 #pragma unroll
-        for (int k = 0; k < UPL; ++k) {
-          acc[k].x |= x[q][k].x;
-          acc[k].y |= x[q][k].y;
-          acc[k].z |= x[q][k].z;
-          acc[k].w |= x[q][k].w;
+        for (int p = 0; p < PPL; ++p) {
+          ggb::or_into(acc[p][0], x[q][p][0]);
+          ggb::or_into(acc[p][1], x[q][p][1]);
         }
     }
 #pragma unroll
-    for (int k = 0; k < UPL; ++k) {
-      __stcg(dst + v * R + li + k * LPR, acc[k]);
-      c += __popc(acc[k].x) + __popc(acc[k].y) + __popc(acc[k].z) + __popc(acc[k].w);
+    for (int p = 0; p < PPL; ++p) {
+      if constexpr (R >= 2) {
+        ggb::st_cg2(dst + v * R + 2 * (li + p * LP), acc[p]);
+      } else {
+        __stcg(dst + v, acc[p][0]);
+      }
+      c += ggb::popc4(acc[p][0]) + ggb::popc4(acc[p][1]);
     }
   }
   if (c == 0xffffffffu) atomicAdd(sink, 1ULL);   // keeps the loads alive
@@ -63,8 +88,9 @@ __global__ void __launch_bounds__(512, 2) probe_gather_kernel(const uint4* __res
 
 template <int R>
 float time_sweeps(uint4* a, uint4* b, const int* adj, int N, int d, int iters, unsigned long long* sink, int sms) {
-  constexpr int VPW = 32 / (R >= 32 ? 32 : R);
-  const long long want = ((long long)N + VPW * 16 - 1) / (VPW * 16);
+  constexpr int PARTS = R >= 2 ? R / 2 : 1;
+  constexpr int RPW = 32 / (PARTS >= 32 ? 32 : PARTS);
+  const long long want = ((long long)N + RPW * 16 - 1) / (RPW * 16);
   const int grid = (int)std::min<long long>(want, 2LL * sms);
   cudaEvent_t e0, e1;
   if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) return -1.f;
@@ -87,12 +113,16 @@ float time_sweeps(uint4* a, uint4* b, const int* adj, int N, int d, int iters, u
 
 }  // namespace
 
-// Gathered GB/s of random-row OR sweeps over an N x (window_bits/8)-byte
-// matrix with d random neighbours per row (a fixed-seed LCG graph), averaged
-// over `iters` sweeps after warm-up, on the current device.
+// GB/s of random-row OR sweeps over an N x (window_bits/8)-byte matrix with d
+// random neighbours per row (a fixed-seed LCG graph), averaged over `iters`
+// sweeps after warm-up, on the current device.  The bytes are counted as the
+// evaluator's algorithmic bytes of one dense sweep are: N*d*4 adjacency +
+// N*d*W/8 gathered rows + 2*N*W/8 own row read and new row written.
 extern "C" int ggb_probe_l2_gather(int N, int d, int window_bits, int iters, double* gbs) {
-  const int R = window_bits / 128;
-  if (N <= 0 || d <= 0 || iters <= 0 || !gbs || window_bits <= 0 || window_bits % 128 || (R & (R - 1)) || R > 64)
+  // 64-source windows use rows of one uint4, as the evaluator does
+  const int R = window_bits == 64 ? 1 : window_bits / 128;
+  if (N <= 0 || d <= 0 || iters <= 0 || !gbs || window_bits <= 0 ||
+      (window_bits != 64 && (window_bits % 128 || (R & (R - 1)) || R > 64)))
     return GGB_EINVAL;
   std::vector<int> adj((size_t)N * d);
   unsigned long long x = 0x9e3779b97f4a7c15ULL;
@@ -135,6 +165,7 @@ extern "C" int ggb_probe_l2_gather(int N, int d, int window_bits, int iters, dou
   cudaFree(buf);
   cudaFree(sink);
   if (e != cudaSuccess || ms <= 0.f) return GGB_ECUDA;
-  *gbs = (double)N * d * 16.0 * R / (ms * 1e-3) / 1e9;
+  const double row = window_bits / 8.0;
+  *gbs = ((double)N * d * 4.0 + (double)N * d * row + 2.0 * N * row) / (ms * 1e-3) / 1e9;
   return GGB_OK;
 }

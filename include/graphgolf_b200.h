@@ -51,7 +51,7 @@ typedef struct ggb_result {
                            `sum += nodes*(nodes-1)`; 0 if disconnected        */
   long long levels;     /* BFS levels executed, summed over source windows   */
   int windows;          /* source windows run                                 */
-  int window_bits;      /* sources per window (a multiple of 128)             */
+  int window_bits;      /* sources per window (64 or a multiple of 128)       */
   long long dense_levels; /* of `levels`, those run as dense OR-gather sweeps
                            (the first two levels of a window are seeded from
                            the two-hop adjacency instead)                     */
@@ -90,9 +90,12 @@ const char *ggb_version(void);
 /* Number of CUDA devices visible to this process (0 if none or on error). */
 int ggb_device_count(void);
 
-/* Forces the source-window width (bits, multiple of 128, 0 = automatic) and
- * the persistent grid size (CTAs, 0 = automatic).  Used by the autotuner and
- * by tests that sweep widths; results never depend on either. */
+/* Forces the source-window width (bits: 64, or 128 * 2^k up to 8192; 0 =
+ * automatic) and the persistent grid size (CTAs, 0 = automatic).  Used by the
+ * autotuner and by tests and benchmarks that sweep widths; results never
+ * depend on either.  64-source windows (the reference's one-word chunk,
+ * general/evaluation.cu:27-44) keep one 16-byte row per vertex with its upper
+ * half zero: a gather fetches one 32-byte L2 sector either way. */
 int ggb_set_tuning(int window_bits, int ctas);
 
 /* Policy for the ball pre-pass (one kernel that writes S_3 of every source
@@ -128,10 +131,13 @@ int ggb_trace_read(long long *out, int max_pairs);
 int ggb_set_timing(int enable);
 int ggb_kernel_times(double *ms_ball, double *ms_persistent);
 
-/* The roof the dense sweeps run against: gathered GB/s of random-row OR
- * sweeps (d random neighbours per row, rows of window_bits/8 bytes, N rows),
- * one launch per sweep, on the current device with its own buffers.  No
- * counterpart in the reference; a measurement utility for the roofline. */
+/* The roof the dense sweeps run against: random-row OR sweeps (d random
+ * neighbours per row, rows of window_bits/8 bytes, N rows) with the sweeps'
+ * own access width (32-byte loads for rows of 32 bytes or more), one launch
+ * per sweep, on the current device with its own buffers.  *gbs counts the
+ * algorithmic bytes of a dense sweep (N*d*4 + N*d*W/8 + 2*N*W/8) per second,
+ * the figure bench.py's roofline reports for the evaluator.  No counterpart
+ * in the reference; a measurement utility for the roofline. */
 int ggb_probe_l2_gather(int N, int d, int window_bits, int iters, double *gbs);
 
 /* ---- host-buffer entry points (copy in, evaluate, copy out) ------------ */

@@ -24,19 +24,36 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 REF_DIR = HERE / "_ref"
-REFERENCE_SRC = Path(os.environ.get("GGB_REFERENCE", "/root/reference"))
 
 _port = None
 _ref_general = None
 _ref_grid = None
 
 
-def build(with_reference: bool | None = None) -> None:
-    """Builds liboracle.so and, if the reference sources exist, _ref/."""
-    if with_reference is None:
-        with_reference = REFERENCE_SRC.exists()
-    targets = ["oracle"] + (["ref"] if with_reference else [])
-    subprocess.run(["make", "-s", "-C", str(HERE), f"REF={REFERENCE_SRC}", *targets], check=True)
+def reference_source() -> Path | None:
+    """The reference source tree: $GGB_REFERENCE, else the tree _ref/ was
+    last built from (recorded in _ref/SOURCE by the Makefile), else None."""
+    env = os.environ.get("GGB_REFERENCE")
+    if env:
+        return Path(env)
+    rec = REF_DIR / "SOURCE"
+    if rec.exists():
+        p = rec.read_text().strip()
+        if p:
+            return Path(p)
+    return None
+
+
+def build(reference: str | os.PathLike | None = None) -> None:
+    """Builds liboracle.so and, when a reference source tree is named
+    (`reference`, else reference_source()) and exists, _ref/ from it."""
+    src = Path(reference) if reference else reference_source()
+    targets = ["oracle"]
+    args = []
+    if src is not None and src.exists():
+        targets.append("ref")
+        args.append(f"REF={src}")
+    subprocess.run(["make", "-s", "-C", str(HERE), *args, *targets], check=True)
 
 
 def port() -> C.CDLL:
@@ -44,7 +61,7 @@ def port() -> C.CDLL:
     if _port is None:
         path = HERE / "liboracle.so"
         if not path.exists():
-            build(with_reference=False)
+            subprocess.run(["make", "-s", "-C", str(HERE), "oracle"], check=True)
         lib = C.CDLL(str(path))
         I, LL, P = C.c_int, C.c_longlong, C.c_void_p
         IP, DP, LP = C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_longlong)
@@ -109,15 +126,20 @@ def general(adj, based_nodes=None, groups=1, added_centers=0, algo=1):
     return bool(rc), dm.value, asp.value, (tot.value if rc else 0)
 
 
-def general_partial(adj, rank, procs, based_nodes=None, groups=1, added_centers=0):
-    """Port: rank's partial (diam, sum) before the MPI_Allreduce."""
+def general_partial(adj, rank, procs, based_nodes=None, groups=1, added_centers=0, window_bits=0):
+    """Port: rank's partial (diam, sum) before the MPI_Allreduce.  With
+    window_bits (a multiple of 64) the source chunks are windows of that many
+    sources instead of the reference's ceil(elements/procs) words, so that the
+    partial can be compared with the GPU partial of the same window width."""
     a = _adj(adj)
     n, d = a.shape
     if based_nodes is None:
         based_nodes = (n - added_centers) // groups
+    if window_bits % 64:
+        raise ValueError("window_bits must be a multiple of 64")
     dm, sm = C.c_int(0), C.c_longlong(0)
-    rc = port().oracle_general_partial(n, based_nodes, groups, d, a.ctypes.data, added_centers, 0, rank, procs,
-                                       C.byref(dm), C.byref(sm))
+    rc = port().oracle_general_partial(n, based_nodes, groups, d, a.ctypes.data, added_centers, window_bits // 64,
+                                       rank, procs, C.byref(dm), C.byref(sm))
     if rc < 0:
         raise ValueError(f"oracle_general_partial: {rc}")
     return dm.value, sm.value

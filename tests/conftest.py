@@ -8,7 +8,6 @@ ROOT = Path(__file__).resolve().parent.parent
 if str(ROOT) not in sys.path:
     sys.path.insert(0, str(ROOT))
 
-REFERENCE = Path(os.environ.get("GGB_REFERENCE", "/root/reference"))
 
 
 def pytest_configure(config):
@@ -20,7 +19,8 @@ def _ensure_built():
     from graphgolf_b200 import build as b
     b.build()
     import oracle
-    if not (oracle.HERE / "liboracle.so").exists() or (REFERENCE.exists() and not oracle.have_ref()):
+    src = oracle.reference_source()
+    if not (oracle.HERE / "liboracle.so").exists() or (src is not None and src.exists() and not oracle.have_ref()):
         oracle.build()
 
 
@@ -43,9 +43,13 @@ def gpu():
 
 @pytest.fixture(scope="session")
 def reference_tree():
-    if not REFERENCE.exists():
-        pytest.skip("reference source tree not present")
-    return REFERENCE
+    """The reference source tree ($GGB_REFERENCE, or the one oracle/_ref was
+    built from); tests that read its own data files skip without it."""
+    import oracle
+    src = oracle.reference_source()
+    if src is None or not src.exists():
+        pytest.skip("reference source tree not present (set GGB_REFERENCE)")
+    return src
 
 
 @pytest.fixture(scope="session")

@@ -107,7 +107,9 @@ def expected(c: dict, adj: np.ndarray, rh) -> dict:
 
 def main() -> None:
     if not oracle.have_ref():
-        oracle.build(with_reference=True)
+        oracle.build()
+    if not oracle.have_ref():
+        raise SystemExit("oracle/_ref is not built: set GGB_REFERENCE to the reference source tree")
     rows = []
     for c in CASES:
         adj, rh = build_case(c)

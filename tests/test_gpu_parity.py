@@ -47,7 +47,7 @@ def test_random_vs_oracle(gpu, n, d, seed):
     assert (r.connected, r.diameter, r.aspl, r.total) == (ok, diam, aspl, total)
 
 
-@pytest.mark.parametrize("bits", [128, 256, 512, 1024, 2048, 4096, 8192])
+@pytest.mark.parametrize("bits", [64, 128, 256, 512, 1024, 2048, 4096, 8192])
 def test_window_width_sweep(gpu, bits):
     """Results never depend on the window width or the grid size."""
     adj = graphs.random_regular(3000, 7, 21).adj
@@ -135,8 +135,34 @@ def test_large_properties(gpu):
             assert r.windows == -(-65536 // c["groups"] // r.window_bits)
 
 
+def _headline_cases():
+    return [c for c in golden_cases() if c["nodes"] == 65536]
+
+
+@pytest.mark.parametrize("bits", [64, 128, 256, 512, 0])
+@pytest.mark.parametrize("c", _headline_cases(), ids=case_id)
+def test_headline_graph_at_every_width(gpu, c, bits):
+    """The single-large-evaluation configuration at its size: the seeded
+    16-regular graph with N=65536 (g=1, all 65536 sources) and its rotationally
+    symmetric variant (g=16, 4096 sources), at source-window widths of 64,
+    128, 256 and 512 bits and the automatic width, against the reference
+    build's own answer (tests/golden)."""
+    adj, rh = build(c)
+    try:
+        gg.set_tuning(bits, 0)
+        r = _gpu(c, adj, rh)
+    finally:
+        gg.set_tuning(0, 0)
+    e = c["expected"]
+    assert (r.connected, r.diameter, r.total) == (e["connected"], e["diameter"], e["total"])
+    assert r.aspl == aspl_of(c)
+    if bits:
+        assert r.window_bits == bits
+    assert r.windows == -(-65536 // c["groups"] // r.window_bits)
+
+
 @pytest.mark.parametrize("ball", [0, 1])
-@pytest.mark.parametrize("bits", [128, 1024, 4096])
+@pytest.mark.parametrize("bits", [64, 128, 1024, 4096])
 @pytest.mark.parametrize("n,d,g,ac", [(3000, 7, 1, 0), (3000, 8, 1, 0), (2400, 12, 4, 0), (1040, 8, 16, 16),
                                       (5000, 5, 1, 100), (700, 32, 1, 0)])
 def test_seeding_paths(gpu, ball, bits, n, d, g, ac):

@@ -11,11 +11,15 @@ pytestmark = pytest.mark.gpu
 
 
 def _exact(g, edges):
+    """(diameter, total) of the edges by the oracle (the CPU restatement of the
+    reference's evaluation()); the GPU evaluator must agree."""
     adj = graphs.create_adj(g.nodes, g.degree, edges)
     h = graphs.Graph(g.nodes, g.degree, edges, adj)
     assert graphs.verify(h) == 0
+    ok, diam, _, total = oracle.general(adj)
     r = gg.evaluate(adj)
-    return r.diameter, r.total
+    assert (r.diameter, r.total) == (diam, total)
+    return diam, total
 
 
 def _check(an, g, st):

@@ -31,3 +31,36 @@ def test_batch_workload_shape():
     assert all(graphs.verify(x) == 0 for x in w)
     again = graphs.batch_workload(candidates=12, degree=12, n_lo=512, n_hi=16384, base_nodes=4096, seed=3)
     assert all(np.array_equal(x.adj, y.adj) for x, y in zip(w, again))
+
+
+def test_pure_python_generators_match_the_c_generators():
+    """oracle.graphgen (used by bench.py's reference arm, which loads none of
+    the package's libraries) draws the identical graphs."""
+    from oracle import graphgen
+    for n, d, s in [(500, 6, 3), (66, 5, 5), (1024, 8, 1), (3000, 7, 21)]:
+        g = graphs.random_regular(n, d, s)
+        e = graphgen.random_regular_edges(n, d, s)
+        assert np.array_equal(e, g.edges)
+        assert np.array_equal(graphgen.create_adj(n, d, e), g.adj)
+    for n, d, gr, s in [(256, 6, 4, 2), (2048, 8, 16, 3)]:
+        assert np.array_equal(graphgen.symmetric_regular_edges(n, d, gr, s), graphs.symmetric_regular(n, d, gr, s).edges)
+
+
+def test_pure_python_generator_reproduces_the_headline_graphs():
+    """The bench graphs (N=65536, d=16, g=1 and g=16) by their golden adjacency hashes."""
+    import json
+    import sys
+    from pathlib import Path
+    from oracle import graphgen
+    gold = Path(__file__).resolve().parent / "golden"
+    sys.path.insert(0, str(gold))
+    from make_golden import adj_hash
+    for c in json.loads((gold / "apsp_golden.json").read_text())["cases"]:
+        if c["nodes"] != 65536:
+            continue
+        p = c["params"]
+        if c["groups"] == 1:
+            e = graphgen.random_regular_edges(p["n"], p["d"], c["seed"])
+        else:
+            e = graphgen.symmetric_regular_edges(p["n"], p["d"], c["groups"], c["seed"])
+        assert adj_hash(graphgen.create_adj(p["n"], p["d"], e)) == c["adj_sha"]

@@ -1,8 +1,9 @@
-"""The multi-rank path on CPU: two gloo ranks each take a strided share of
-the source chunks and join the partial results with the all-reduces of
-graphgolf_b200.distributed.  The per-rank partial here is the oracle's (the
-reference's MPI split restated), standing in for the GPU partial; what is
-under test is the host-side decomposition and reduction, which must give the
+"""The multi-rank path: two gloo ranks each take a strided share of the source
+chunks and join the partial results with the all-reduces of
+graphgolf_b200.distributed.  On the CPU the per-rank partial is the oracle's
+(the reference's MPI split restated), standing in for the GPU partial, so
+what is under test is the host-side decomposition and reduction; with a GPU
+the same run uses the CUDA partials.  Either way the result must be the
 one-rank answer exactly.  Also checks that a rank that never joins makes the
 others fail with an error instead of hanging."""
 import os
@@ -30,7 +31,22 @@ def _oracle_partial(adj, rank, procs, based_nodes=None, groups=1, added_centers=
     return ggb_partial(diam, 1 if diam > adj.shape[0] else 0, s, 0, 0, 0, 0)
 
 
-def _worker(rank, world, port, cases, out):
+def _gpu_partial_in_turn(adj, rank, procs, **kw):
+    """The GPU partial of this rank (ggb_eval_general_partial on cuda:0).
+    The ranks share one GPU here, so they take turns, each finishing its
+    evaluation before the next starts; no kernel ever waits on another
+    rank's."""
+    import torch.distributed as dist
+    from graphgolf_b200.evaluator import evaluate_partial
+    p = None
+    for r in range(procs):
+        if r == rank:
+            p = evaluate_partial(adj, rank, procs, **kw)
+        dist.barrier()
+    return p
+
+
+def _worker(rank, world, port, cases, out, use_gpu=False):
     import sys
     sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
     import torch.distributed as dist
@@ -42,18 +58,33 @@ def _worker(rank, world, port, cases, out):
     for adj, g, ac in cases:
         n = adj.shape[0]
         r = evaluate_sharded(adj, based_nodes=(n - ac) // g, groups=g, added_centers=ac,
-                             partial_fn=_oracle_partial)
+                             partial_fn=_gpu_partial_in_turn if use_gpu else _oracle_partial)
         res.append((r.connected, r.diameter, r.aspl, r.total))
     out[rank] = res
     dist.barrier()
     dist.destroy_process_group()
 
 
+def _cases():
+    return [(graphs.random_regular(700, 6, 1).adj, 1, 0),
+            (graphs.symmetric_regular(1024, 8, 4, 2).adj, 4, 0),
+            (graphs.random_regular(610, 5, 3).adj, 2, 10)]
+
+
 def test_two_gloo_ranks_match_one_rank():
+    _run_two_ranks(use_gpu=False)
+
+
+@pytest.mark.gpu
+def test_two_gloo_ranks_with_gpu_partials_match_one_rank(gpu):
+    """The same decomposition with each rank's partial computed by the CUDA
+    path (ggb_eval_general_partial) instead of the oracle's."""
+    _run_two_ranks(use_gpu=True)
+
+
+def _run_two_ranks(use_gpu):
     import oracle
-    cases = [(graphs.random_regular(700, 6, 1).adj, 1, 0),
-             (graphs.symmetric_regular(1024, 8, 4, 2).adj, 4, 0),
-             (graphs.random_regular(610, 5, 3).adj, 2, 10)]
+    cases = _cases()
     want = []
     for adj, g, ac in cases:
         n = adj.shape[0]
@@ -62,7 +93,7 @@ def test_two_gloo_ranks_match_one_rank():
     mgr = ctx.Manager()
     out = mgr.dict()
     port = _free_port()
-    procs = [ctx.Process(target=_worker, args=(r, 2, port, cases, out)) for r in range(2)]
+    procs = [ctx.Process(target=_worker, args=(r, 2, port, cases, out, use_gpu)) for r in range(2)]
     for p in procs:
         p.start()
     for p in procs:

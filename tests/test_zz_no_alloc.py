@@ -15,6 +15,7 @@ import numpy as np
 import pytest
 
 import graphgolf_b200 as gg
+import oracle
 from graphgolf_b200 import _native, graphs
 
 pytestmark = pytest.mark.gpu
@@ -33,6 +34,7 @@ def test_no_alloc_matches_device_entry(gpu, n, d, g, ac, seed):
     adj_dev = torch.from_numpy(np.ascontiguousarray(adj)).cuda()
     torch.cuda.synchronize()
     bn = (n - ac) // g
+    want = oracle.general(adj, groups=g, added_centers=ac)   # the CPU restatement of the reference
     ref = _native.ggb_result()
     assert lib.ggb_eval_general_device(n, bn, g, d, adj_dev.data_ptr(), ac, None, C.byref(ref)) == 0, \
         _native.last_error()
@@ -43,6 +45,7 @@ def test_no_alloc_matches_device_entry(gpu, n, d, g, ac, seed):
         # integers bit-exact, ASPL the identical double (the tolerance of every parity test here)
         assert (out.connected, out.diameter, out.total) == (ref.connected, ref.diameter, ref.total)
         assert out.aspl == ref.aspl
+        assert (bool(out.connected), out.diameter, out.aspl, out.total) == want
 
 
 def test_no_alloc_rejects_too_large(gpu):
@@ -54,3 +57,7 @@ def test_no_alloc_rejects_too_large(gpu):
     rc = lib.ggb_eval_general_noalloc(1 << 20, 1 << 20, 1, 4, dummy.data_ptr(), 0, None, C.byref(out))
     assert rc == -1
     assert b"too large" in lib.ggb_noalloc_last_error()
+    # few enough vertices for the array, but more adjacency entries than an int32 offset reaches
+    rc = lib.ggb_eval_general_noalloc(200000, 200000, 1, 20000, dummy.data_ptr(), 0, None, C.byref(out))
+    assert rc == -1
+    assert b"int32" in lib.ggb_noalloc_last_error()
