@@ -125,6 +125,8 @@ CORE_SIGNATURES = {
     "ggb_mlp_grads_host": (_I, [_P, _P, _P, _I, _P, _P]),
     "ggb_mlp_train_host": (_I, [_P, _P, _P, _I, _I, _P]),
     "ggb_sa_create": (_I, [_I, _I, _P, _I, _I, _I, C.c_ulonglong, C.POINTER(_P)]),
+    "ggb_sa_create_symmetric": (_I, [_I, _I, _I, _P, _I, _I, C.c_ulonglong, C.POINTER(_P)]),
+    "ggb_sa_set_grid": (_I, [_P, _I, _I]),
     "ggb_sa_destroy": (None, [_P]),
     "ggb_sa_set_schedule": (_I, [_P, C.c_double, C.c_double, _I]),
     "ggb_sa_set_target": (_I, [_P, _I, _LL]),

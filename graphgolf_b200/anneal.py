@@ -42,17 +42,26 @@ class Stats:
 
 
 class Annealer:
+    """Device annealing of `g`.  With g.groups > 1 (edges in the reference's
+    symmetric line order) every move is an orbit move that keeps the symmetry
+    and there is no proposal filter; grid graphs add a length limit with
+    ``grid()``."""
+
     def __init__(self, g: Graph, candidates: int = 1, proposals: int | None = None, compose: int = 0,
                  seed: int = 1):
-        if g.groups != 1:
-            raise ValueError("device annealing takes graphs without symmetry groups")
         self._lib = load()
-        self.nodes, self.degree, self.lines = g.nodes, g.degree, g.lines
+        self.nodes, self.degree, self.lines, self.groups = g.nodes, g.degree, g.lines, g.groups
         self.candidates = candidates
         e = np.ascontiguousarray(g.edges, dtype=np.int32)
         h = C.c_void_p()
-        _raise(self._lib.ggb_sa_create(g.nodes, g.degree, e.ctypes.data, candidates,
-                                       proposals if proposals else candidates, compose, seed, C.byref(h)))
+        if g.groups > 1:
+            if proposals not in (None, candidates):
+                raise ValueError("graphs with symmetry groups are annealed without a proposal filter")
+            _raise(self._lib.ggb_sa_create_symmetric(g.nodes, g.degree, g.groups, e.ctypes.data, candidates,
+                                                     compose, seed, C.byref(h)))
+        else:
+            _raise(self._lib.ggb_sa_create(g.nodes, g.degree, e.ctypes.data, candidates,
+                                           proposals if proposals else candidates, compose, seed, C.byref(h)))
         self._h = h
 
     def close(self) -> None:
@@ -74,6 +83,11 @@ class Annealer:
 
     def schedule(self, temp: float = 0.0, cooling: float = 1.0, hill_climbing: bool = True) -> None:
         _raise(self._lib.ggb_sa_set_schedule(self._h, temp, cooling, 1 if hill_climbing else 0))
+
+    def grid(self, height: int, max_length: int) -> None:
+        """Grid graph: vertex v = (v // height, v % height); every move keeps
+        both new edges within Manhattan length max_length (grid/sa.c:137-221)."""
+        _raise(self._lib.ggb_sa_set_grid(self._h, height, max_length))
 
     def predicted(self, composites: int = 4, max_swaps: int = 64) -> None:
         """Predicted composites per step (filter only) and the largest's size."""

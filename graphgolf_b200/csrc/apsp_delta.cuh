@@ -38,12 +38,16 @@ namespace ggb {
 // line[1] = {x2,x3} become {x0,x2} and {x1,x3}.  pos[k] is the slot of row
 // x_k whose entry changes: row x0: x1 -> x2, row x1: x0 -> x3,
 // row x2: x3 -> x0, row x3: x2 -> x1.  A valid swap has 4 distinct endpoints.
+// On a graph with symmetry groups (the annealer's orbit moves) the swap is
+// applied to every copy of the two lines (kind 0), or it re-pairs the edge
+// orbit of line[0] = {x0,x1} with shift x2 (kind 1, x3 unused); pos is then
+// unused and each copy's slot is found by value.
 struct Swap {
   int line[2];
   int x[4];
   int pos[4];
   int valid;
-  int pad_;
+  int kind;
 };
 
 // ---- the base build: one graph, windows split over CTA teams, levels kept ------

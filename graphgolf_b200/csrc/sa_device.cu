@@ -82,6 +82,14 @@ struct State {
   int stop_on_target;
   unsigned long long seed;
   float label_scale, label_clip;
+  // Symmetry groups: the graph is invariant under v -> v + B (mod N), B = N / groups,
+  // and line k*BL + i is line i shifted by k*B (BL = lines / groups), the
+  // reference's symmetric line order (general/main.c:175-183).  groups = 1: none.
+  int groups, B, BL;
+  // Grid graphs: vertex v = x*grid_height + y on the lattice; every new edge
+  // must stay within Manhattan length grid_length (0: no length limit).
+  int grid_height, grid_length;
+  int move_error;        // a move's old neighbour was not found where the state says (never expected)
 };
 
 constexpr unsigned long long kGolden = 0x9e3779b97f4a7c15ULL;
@@ -109,25 +117,88 @@ __device__ __forceinline__ int find_in_row(const int* row, int d, int x) {
 }
 
 // ---- gen: candidate swaps ------------------------------------------------------
+__device__ __forceinline__ int manhattan(int v, int w, int H) {
+  const int dx = v / H - w / H, dy = v % H - w % H;
+  return (dx < 0 ? -dx : dx) + (dy < 0 ? -dy : dy);
+}
+
+// v shifted by k copies: v + k*B (mod N), 0 <= v < N, -groups < k < 2*groups.
+__device__ __forceinline__ int shift_copy(const State* s, int v, int k) {
+  long long y = (long long)v + (long long)k * s->B;
+  y %= s->N;
+  if (y < 0) y += s->N;
+  return (int)y;
+}
+
+// An orbit move of a graph with symmetry groups (general/sa.c:217-369 and
+// general/common.c:162-276, restated for the device): two random lines; when
+// they lie in the same orbit (their indices agree modulo BL) the orbit's edges
+// {x0 + kB, x1 + kB} are re-paired as {x0 + kB, x1 + (k + p)B} for a random
+// shift p in [1, groups) (1g-opt), otherwise the two lines and all their copies
+// are swapped alike (2g-opt).  The endpoints' classes (v mod B) must be
+// pairwise distinct, so that every changed row changes once and no orbit
+// repeats or loses an edge; a new edge must not exist yet.  Both keep the
+// graph simple, regular and symmetric.
+__device__ bool gen_orbit_move(const State* s, unsigned long long h, Swap& w) {
+  const int lines = s->lines, d = s->d, B = s->B;
+  const int* __restrict__ E = s->edges;
+  const int* __restrict__ A = s->adj;
+  const int i = below(h, lines), j = below(h << 32, lines);
+  if (i == j) return false;
+  const int a = E[2 * i], b = E[2 * i + 1];
+  if (a % B == b % B) return false;
+  if ((i - j) % s->BL == 0) {
+    const int p = 1 + below(mix64(h ^ 0x6a09e667f3bcc909ULL), s->groups - 1);
+    const int bp = shift_copy(s, b, p);
+    if (find_in_row(A + (long long)a * d, d, bp) >= 0) return false;
+    w.kind = 1;
+    w.line[0] = i; w.line[1] = i;
+    w.x[0] = a; w.x[1] = b; w.x[2] = p; w.x[3] = -1;
+    return true;
+  }
+  const int r = (int)(mix64(h) & 1);
+  const int c = E[2 * j], e = E[2 * j + 1];
+  const int x0 = a, x1 = b, x2 = r ? e : c, x3 = r ? c : e;
+  const int c0 = x0 % B, c1 = x1 % B, c2 = x2 % B, c3 = x3 % B;
+  if (c0 == c2 || c0 == c3 || c1 == c2 || c1 == c3 || c2 == c3) return false;
+  if (find_in_row(A + (long long)x0 * d, d, x2) >= 0 || find_in_row(A + (long long)x1 * d, d, x3) >= 0)
+    return false;
+  w.kind = 0;
+  w.line[0] = i; w.line[1] = j;
+  w.x[0] = x0; w.x[1] = x1; w.x[2] = x2; w.x[3] = x3;
+  return true;
+}
+
 __global__ void gen_kernel(const State* __restrict__ s, Swap* __restrict__ out, int G) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= G) return;
   Swap w;
   w.valid = 0;
-  w.pad_ = 0;
+  w.kind = 0;
   if (!s->done) {
     const int lines = s->lines, d = s->d;
     const int* __restrict__ E = s->edges;
     const int* __restrict__ A = s->adj;
     const unsigned long long seed = s->seed, step = (unsigned long long)s->step;
-    for (int attempt = 0; attempt < 64 && !w.valid; ++attempt) {
+    // a length limit rejects most random pairs of lines (both new edges must be
+    // short): draw more of them; the length test comes before any row scan
+    const int attempts = s->grid_length > 0 ? 1024 : 64;
+    for (int attempt = 0; attempt < attempts && !w.valid; ++attempt) {
       const unsigned long long h = draw(seed, step, (unsigned long long)k, (unsigned long long)attempt);
+      if (s->groups > 1) {
+        if (gen_orbit_move(s, h, w)) w.valid = 1;
+        continue;
+      }
       const int i = below(h, lines), j = below(h << 32, lines);
       if (i == j) continue;
       const int r = (int)(mix64(h) & 1);
       const int a = E[2 * i], b = E[2 * i + 1], c = E[2 * j], e = E[2 * j + 1];
       const int x0 = a, x1 = b, x2 = r ? e : c, x3 = r ? c : e;
       if (x0 == x2 || x1 == x3) continue;
+      // grid graphs: both new edges within the length limit (grid/sa.c:196-201)
+      if (s->grid_length > 0 && (manhattan(x0, x2, s->grid_height) > s->grid_length ||
+                                 manhattan(x1, x3, s->grid_height) > s->grid_length))
+        continue;
       const int* r0 = A + (long long)x0 * d;
       const int* r1 = A + (long long)x1 * d;
       if (find_in_row(r0, d, x2) >= 0 || find_in_row(r1, d, x3) >= 0) continue;
@@ -156,7 +227,7 @@ __global__ void materialize_kernel(const State* __restrict__ s, const Swap* __re
   const long long n = (long long)s->N * d;
   long long off[4] = {-1, -1, -1, -1};
   int val[4] = {0, 0, 0, 0};
-  if (w.valid) {
+  if (w.valid && s->groups == 1) {   // orbit moves are patched by patch_orbit_kernel
     const int nv[4] = {w.x[2], w.x[3], w.x[0], w.x[1]};
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
@@ -173,6 +244,108 @@ __global__ void materialize_kernel(const State* __restrict__ s, const Swap* __re
       if (i == off[q]) v = val[q];
     dst[i] = v;
   }
+}
+
+__device__ __forceinline__ void apply_swap(int* adj, int d, const Swap& w) {
+  adj[(long long)w.x[0] * d + w.pos[0]] = w.x[2];
+  adj[(long long)w.x[1] * d + w.pos[1]] = w.x[3];
+  adj[(long long)w.x[2] * d + w.pos[2]] = w.x[0];
+  adj[(long long)w.x[3] * d + w.pos[3]] = w.x[1];
+}
+
+// In row v, the entry equal to `from` becomes `to`; false if there is none.
+__device__ __forceinline__ bool replace_in_row(int* adj, int d, int v, int from, int to) {
+  int* row = adj + (long long)v * d;
+  const int j = find_in_row(row, d, from);
+  if (j < 0) return false;
+  row[j] = to;
+  return true;
+}
+
+// Applies one move to `adj` and, when given, to the edge list in the
+// symmetric line order.  Copy k of an orbit move changes the rows of the
+// endpoints shifted by k*B; their classes are distinct (gen_orbit_move), so
+// every changed row changes once and the copies can be found by value.
+// Returns false if an old neighbour was missing (a state inconsistency).
+__device__ bool apply_move(const State* s, int* adj, int* edges, const Swap& w) {
+  const int d = s->d;
+  if (s->groups == 1) {
+    apply_swap(adj, d, w);
+    if (edges) {
+      edges[2 * w.line[0]] = w.x[0];
+      edges[2 * w.line[0] + 1] = w.x[2];
+      edges[2 * w.line[1]] = w.x[1];
+      edges[2 * w.line[1] + 1] = w.x[3];
+    }
+    return true;
+  }
+  bool ok = true;
+  for (int k = 0; k < s->groups; ++k) {
+    if (w.kind == 1) {
+      const int p = w.x[2];
+      const int va = shift_copy(s, w.x[0], k), vb = shift_copy(s, w.x[1], k);
+      const int nb = shift_copy(s, w.x[1], k + p), na = shift_copy(s, w.x[0], k - p);
+      ok &= replace_in_row(adj, d, va, vb, nb);
+      ok &= replace_in_row(adj, d, vb, va, na);
+      if (edges) {
+        const int l = (int)(((long long)w.line[0] + (long long)k * s->BL) % s->lines);
+        edges[2 * l] = va;
+        edges[2 * l + 1] = nb;
+      }
+    } else {
+      const int v0 = shift_copy(s, w.x[0], k), v1 = shift_copy(s, w.x[1], k);
+      const int v2 = shift_copy(s, w.x[2], k), v3 = shift_copy(s, w.x[3], k);
+      ok &= replace_in_row(adj, d, v0, v1, v2);
+      ok &= replace_in_row(adj, d, v1, v0, v3);
+      ok &= replace_in_row(adj, d, v2, v3, v0);
+      ok &= replace_in_row(adj, d, v3, v2, v1);
+      if (edges) {
+        const int l0 = (int)(((long long)w.line[0] + (long long)k * s->BL) % s->lines);
+        const int l1 = (int)(((long long)w.line[1] + (long long)k * s->BL) % s->lines);
+        edges[2 * l0] = v0;
+        edges[2 * l0 + 1] = v2;
+        edges[2 * l1] = v1;
+        edges[2 * l1 + 1] = v3;
+      }
+    }
+  }
+  return ok;
+}
+
+// The vertex classes (v mod B; the vertices themselves without symmetry) a
+// move touches: moves with disjoint classes change disjoint rows and can be
+// applied together.  Returns how many of out[0..4) it wrote.
+__device__ __forceinline__ int move_classes(const State* s, const Swap& w, int* out) {
+  if (s->groups > 1 && w.kind == 1) {
+    out[0] = w.x[0] % s->B;
+    out[1] = w.x[1] % s->B;
+    return 2;
+  }
+  for (int q = 0; q < 4; ++q) out[q] = s->groups > 1 ? w.x[q] % s->B : w.x[q];
+  return 4;
+}
+
+__device__ __forceinline__ bool classes_free(const unsigned* vmark, const int* c, int n) {
+  bool f = true;
+  for (int q = 0; q < n; ++q) f &= !((vmark[c[q] >> 5] >> (c[q] & 31)) & 1u);
+  return f;
+}
+
+__device__ __forceinline__ void classes_set(unsigned* vmark, const int* c, int n, bool on) {
+  for (int q = 0; q < n; ++q) {
+    if (on) vmark[c[q] >> 5] |= 1u << (c[q] & 31);
+    else vmark[c[q] >> 5] = 0u;
+  }
+}
+
+// Orbit moves of the candidates: slot k (block k) = the current adjacency,
+// copied by materialize_kernel, with candidate sel[k]'s move applied.
+__global__ void patch_orbit_kernel(State* __restrict__ s, const Swap* __restrict__ sw, const int* __restrict__ sel,
+                                   int* __restrict__ slots, long long slot_stride) {
+  if (s->done || s->groups == 1 || threadIdx.x != 0) return;
+  const int k = blockIdx.x;
+  const Swap w = sw[sel ? sel[k] : k];
+  if (w.valid && !apply_move(s, slots + (long long)k * slot_stride, nullptr, w)) atomicExch(&s->move_error, 1);
 }
 
 struct Key {
@@ -192,6 +365,18 @@ __device__ __forceinline__ Key key_of(const BatchOut& o, int N) {
   return k;
 }
 
+// Key of candidate k: a candidate whose draw found no valid move (its slot
+// holds the unchanged graph) never competes.
+__device__ __forceinline__ Key cand_key(const Swap* sw, const int* sel, const BatchOut* out, int k, int N) {
+  if (!sw[sel ? sel[k] : k].valid) {
+    Key no;
+    no.diam = INT_MAX;
+    no.total = LLONG_MAX;
+    return no;
+  }
+  return key_of(out[k], N);
+}
+
 __device__ __forceinline__ bool key_less(const Key& a, const Key& b) {
   return a.diam < b.diam || (a.diam == b.diam && a.total < b.total);
 }
@@ -209,7 +394,7 @@ __global__ void __launch_bounds__(kComposeThreads) compose_kernel(State* __restr
   if (s->done) return;
   const int N = s->N;
   const int k = threadIdx.x;
-  if (k < K) s_keys[k] = key_of(out[k], N);
+  if (k < K) s_keys[k] = cand_key(sw, sel, out, k, N);
   __syncthreads();
   if (k < K) {
     const Key me = s_keys[k];
@@ -232,32 +417,30 @@ __global__ void __launch_bounds__(kComposeThreads) compose_kernel(State* __restr
     if (!key_less(kc, cur)) break;   // sorted: nothing further improves
     const Swap w = sw[sel ? sel[c] : c];
     if (!w.valid) continue;
-    bool free_ = true;
-    for (int q = 0; q < 4; ++q) free_ &= !((vmark[w.x[q] >> 5] >> (w.x[q] & 31)) & 1u);
-    if (!free_) continue;
-    for (int q = 0; q < 4; ++q) vmark[w.x[q] >> 5] |= 1u << (w.x[q] & 31);
+    int cl[4];
+    const int nc = move_classes(s, w, cl);
+    if (!classes_free(vmark, cl, nc)) continue;
+    classes_set(vmark, cl, nc, true);
     comp[m++] = w;
   }
-  for (int i = 0; i < m; ++i)
-    for (int q = 0; q < 4; ++q) vmark[comp[i].x[q] >> 5] = 0u;
+  for (int i = 0; i < m; ++i) {
+    int cl[4];
+    const int nc = move_classes(s, comp[i], cl);
+    classes_set(vmark, cl, nc, false);
+  }
   s->n_comp = m;
 }
 
 // Size of predicted composite c: the first n_pred >> c swaps of the list.
 __device__ __forceinline__ int pred_size(int n_pred, int c) { return n_pred >> c; }
 
-__device__ __forceinline__ void apply_swap(int* adj, int d, const Swap& w) {
-  adj[(long long)w.x[0] * d + w.pos[0]] = w.x[2];
-  adj[(long long)w.x[1] * d + w.pos[1]] = w.x[3];
-  adj[(long long)w.x[2] * d + w.pos[2]] = w.x[0];
-  adj[(long long)w.x[3] * d + w.pos[3]] = w.x[1];
-}
 
 
 // ---- decide ---------------------------------------------------------------------------
-// general/sa.c:371-411 on exact totals: with groups = 1 the reference's
-// diff = (current_ASPL - new_ASPL) * N(N-1) is the change of the distance
-// total.  Threads k < K also write the training labels of this step.
+// general/sa.c:371-411 on exact totals: the reference's
+// diff = (current_ASPL - new_ASPL) * N(N-1) / groups is the change of the
+// (group-weighted) distance total divided by groups.  Threads k < K also
+// write the training labels of this step.
 // comp_out (when there is a composite batch): [0] the exact composite,
 // [1 + c] predicted composite c.
 __global__ void decide_kernel(State* __restrict__ s, const Swap* __restrict__ sw, const int* __restrict__ sel,
@@ -280,7 +463,7 @@ __global__ void decide_kernel(State* __restrict__ s, const Swap* __restrict__ sw
   if (k != 0) return;
   const Key cur = {s->cur_diam, s->cur_total};
   const int bk = s->best_k;
-  Key cand = key_of(out[bk], N);
+  Key cand = cand_key(sw, sel, out, bk, N);
   bool use_comp = false;
   int use_pred = 0;   // swaps of the chosen predicted composite (0: none)
   if (comp_out && s->n_comp >= 2) {
@@ -308,7 +491,7 @@ __global__ void decide_kernel(State* __restrict__ s, const Swap* __restrict__ sw
       if (cand.total <= cur.total) {
         acc = true;
       } else if (!s->hill) {
-        const double diff = (double)(cur.total - cand.total);
+        const double diff = (double)(cur.total - cand.total) / (double)s->groups;
         const unsigned long long h = draw(s->seed ^ 0x5bd1e995ULL, (unsigned long long)s->step, 0x0dec1deULL, 7);
         const double u = ((double)(h >> 11) + 1.0) / (9007199254740992.0 + 2.0);
         acc = exp(diff / s->temp) > u;
@@ -317,39 +500,21 @@ __global__ void decide_kernel(State* __restrict__ s, const Swap* __restrict__ sw
   }
   s->evals += K + C + (comp_out ? 1 : 0);
   if (acc) {
-    const int d = s->d;
+    bool ok = true;
     if (use_pred) {
-      for (int i = 0; i < use_pred; ++i) {
-        const Swap& w = pred[i];
-        apply_swap(s->adj, d, w);
-        s->edges[2 * w.line[0]] = w.x[0];
-        s->edges[2 * w.line[0] + 1] = w.x[2];
-        s->edges[2 * w.line[1]] = w.x[1];
-        s->edges[2 * w.line[1] + 1] = w.x[3];
-      }
+      for (int i = 0; i < use_pred; ++i) ok &= apply_move(s, s->adj, s->edges, pred[i]);
       s->multi_accepts += 1;
       s->pred_accepts += 1;
       s->moved_swaps += use_pred;
     } else if (use_comp) {
-      for (int i = 0; i < s->n_comp; ++i) {
-        const Swap& w = comp[i];
-        apply_swap(s->adj, d, w);
-        s->edges[2 * w.line[0]] = w.x[0];
-        s->edges[2 * w.line[0] + 1] = w.x[2];
-        s->edges[2 * w.line[1]] = w.x[1];
-        s->edges[2 * w.line[1] + 1] = w.x[3];
-      }
+      for (int i = 0; i < s->n_comp; ++i) ok &= apply_move(s, s->adj, s->edges, comp[i]);
       s->multi_accepts += 1;
       s->moved_swaps += s->n_comp;
     } else {
-      const Swap w = sw[sel ? sel[bk] : bk];
-      apply_swap(s->adj, d, w);
-      s->edges[2 * w.line[0]] = w.x[0];
-      s->edges[2 * w.line[0] + 1] = w.x[2];
-      s->edges[2 * w.line[1]] = w.x[1];
-      s->edges[2 * w.line[1] + 1] = w.x[3];
+      ok &= apply_move(s, s->adj, s->edges, sw[sel ? sel[bk] : bk]);
       s->moved_swaps += 1;
     }
+    if (!ok) s->move_error = 1;
     s->accepts += 1;
     s->cur_diam = cand.diam;
     s->cur_total = cand.total;
@@ -522,14 +687,17 @@ __global__ void pred_list_kernel(State* __restrict__ s, const Swap* __restrict__
     if (!(rank_key[r] < 0.f)) break;   // sorted: no further predicted gain
     const Swap w = sw[rank[r]];
     if (!w.valid) continue;
-    bool free_ = true;
-    for (int q = 0; q < 4; ++q) free_ &= !((vmark[w.x[q] >> 5] >> (w.x[q] & 31)) & 1u);
-    if (!free_) continue;
-    for (int q = 0; q < 4; ++q) vmark[w.x[q] >> 5] |= 1u << (w.x[q] & 31);
+    int cl[4];
+    const int nc = move_classes(s, w, cl);
+    if (!classes_free(vmark, cl, nc)) continue;
+    classes_set(vmark, cl, nc, true);
     pred[m++] = w;
   }
-  for (int i = 0; i < m; ++i)
-    for (int q = 0; q < 4; ++q) vmark[pred[i].x[q] >> 5] = 0u;
+  for (int i = 0; i < m; ++i) {
+    int cl[4];
+    const int nc = move_classes(s, pred[i], cl);
+    classes_set(vmark, cl, nc, false);
+  }
   s->n_pred = m;
 }
 
@@ -544,7 +712,7 @@ __global__ void copy_composites_kernel(const State* __restrict__ s, int* __restr
     dst[i] = s->adj[i];
 }
 
-__global__ void patch_composites_kernel(const State* __restrict__ s, const Swap* __restrict__ comp,
+__global__ void patch_composites_kernel(State* __restrict__ s, const Swap* __restrict__ comp,
                                         const Swap* __restrict__ pred, int* __restrict__ slots,
                                         long long slot_stride) {
   if (s->done) return;
@@ -552,7 +720,9 @@ __global__ void patch_composites_kernel(const State* __restrict__ s, const Swap*
   int* dst = slots + (long long)slot * slot_stride;
   const Swap* list = slot == 0 ? comp : pred;
   const int m = slot == 0 ? s->n_comp : pred_size(s->n_pred, slot - 1);
-  for (int i = threadIdx.x; i < m; i += blockDim.x) apply_swap(dst, s->d, list[i]);
+  // the moves of a list touch disjoint vertex classes: they change disjoint rows
+  for (int i = threadIdx.x; i < m; i += blockDim.x)
+    if (!apply_move(s, dst, nullptr, list[i])) atomicExch(&s->move_error, 1);
 }
 
 }  // namespace sa
@@ -565,6 +735,7 @@ struct ggb_sa {
   int device = -1;
   int sms = 0;
   int N = 0, d = 0, lines = 0;
+  int groups = 1;                 // symmetry groups: orbit moves, full evaluation of N/groups sources
   int K = 0, G = 0, n_rand = 0, compose_max = 0;
   int C = 0, pred_max = 0;        // predicted composites (learned mode) and their largest size
   bool learned = false;
@@ -663,9 +834,9 @@ ggb::ApspArgs graph_args(ggb_sa* a) {
   p.timeout_ns = 2000000000LL;
   p.N = a->N;
   p.d = a->d;
-  p.n_src1 = a->N;
+  p.n_src1 = a->N / a->groups;
   p.split = a->N;
-  p.groups = 1;
+  p.groups = a->groups;
   p.win_first = 0;
   p.win_stride = 1;
   p.vec4 = (a->d % 4 == 0) ? 1 : 0;
@@ -827,6 +998,10 @@ int enqueue_step(ggb_sa* a, cudaStream_t st) {
     const long long stride = a->cand->off.size() > 1 ? a->cand->off[1] - a->cand->off[0] : 0;
     const int bx = std::max(1, std::min(a->sms * 4 / std::max(a->K, 1), (int)(((long long)a->N * a->d + 255) / 256)));
     materialize_kernel<<<dim3(bx, a->K), 256, 0, st>>>(s, a->d_swaps, sel, a->cand->d_adj, stride);
+    if (a->groups > 1) {
+      patch_orbit_kernel<<<a->K, 32, 0, st>>>(s, a->d_swaps, sel, a->cand->d_adj, stride);
+      launches += 1;
+    }
     rc = ggb::batch_enqueue(a->cand, st);
     if (rc) return rc;
     singles = a->cand->d_out;
@@ -1045,16 +1220,19 @@ int alloc_base(ggb_sa* a) {
   return GGB_OK;
 }
 
-int create(ggb_sa* a, int nodes, int degree, const int* edges, int K, int G, int compose_max,
+int create(ggb_sa* a, int nodes, int degree, int groups, const int* edges, int K, int G, int compose_max,
            unsigned long long seed) {
   using namespace ggb::sa;
   a->N = nodes;
   a->d = degree;
+  a->groups = groups;
   a->lines = (int)((long long)nodes * degree / 2);
   a->K = K;
   a->G = G;
   a->learned = G > K;
-  a->delta = K > 1 && degree <= 32;   // the endpoint search hands neighbour ids over by warp shuffle
+  // the endpoint search hands neighbour ids over by warp shuffle; orbit moves
+  // change 4*groups rows, which the delta path does not serve
+  a->delta = K > 1 && degree <= 32 && groups == 1;
   a->compose_max = compose_max;
   a->n_rand = a->learned ? std::max(1, K / 4) : 0;
   a->C = a->learned ? 4 : 0;
@@ -1077,6 +1255,16 @@ int create(ggb_sa* a, int nodes, int degree, const int* edges, int K, int G, int
       if (adj[(size_t)u * degree + j] == v) return core_fail(GGB_EINVAL, "line %d repeats an edge", i);
     adj[(size_t)u * degree + fill[u]++] = v;
     adj[(size_t)v * degree + fill[v]++] = u;
+  }
+  if (groups > 1) {
+    // the reference's symmetric line order: line k*BL + i is line i shifted by k*B
+    const int B = nodes / groups, BL = a->lines / groups;
+    for (int l = BL; l < a->lines; ++l) {
+      const int i = l % BL, k = l / BL;
+      if (edges[2 * l] != (edges[2 * i] + k * B) % nodes || edges[2 * l + 1] != (edges[2 * i + 1] + k * B) % nodes)
+        return core_fail(GGB_EINVAL, "line %d is not line %d shifted by %d*%d: not in the symmetric line order", l,
+                         i, k, B);
+    }
   }
   int rc;
   const size_t L2 = (size_t)2 * a->lines;
@@ -1143,7 +1331,7 @@ int create(ggb_sa* a, int nodes, int degree, const int* edges, int K, int G, int
   // the candidate batch (full mode) and the composite batch
   const int nc = 1 + a->C;
   const int nmax = std::max(K, nc);
-  std::vector<int> nn(nmax, nodes), bn(nmax, nodes), gg(nmax, 1), dd(nmax, degree);
+  std::vector<int> nn(nmax, nodes), bn(nmax, nodes / groups), gg(nmax, groups), dd(nmax, degree);
   if (!a->delta) {
     if ((rc = ggb_batch_create(K, nn.data(), bn.data(), gg.data(), dd.data(), &a->cand))) return rc;
     a->cand->stop = &a->d_state->done;
@@ -1175,6 +1363,12 @@ int create(ggb_sa* a, int nodes, int degree, const int* edges, int K, int G, int
   a->h.target_total = LLONG_MIN;
   a->h.label_scale = 16.0f / (float)nodes;
   a->h.label_clip = 16.0f;
+  a->h.groups = groups;
+  a->h.B = nodes / groups;
+  a->h.BL = a->lines / groups;
+  a->h.grid_height = 0;
+  a->h.grid_length = 0;
+  a->h.move_error = 0;
   if ((rc = push_state(a))) return rc;
   if (a->has_base && (rc = tune_base(a))) return rc;
   if ((rc = evaluate_current(a))) return rc;
@@ -1239,13 +1433,57 @@ int ggb_sa_create(int nodes, int degree, const int* edges, int candidates, int p
   }
   if (compose_max < 0 || compose_max > 4096) return core_fail(GGB_EINVAL, "compose_max must be in [0, 4096]");
   ggb_sa* a = new ggb_sa();
-  int rc = create(a, nodes, degree, edges, candidates, proposals, compose_max, seed);
+  int rc = create(a, nodes, degree, 1, edges, candidates, proposals, compose_max, seed);
   if (rc) {
     destroy(a);
     return rc;
   }
   *out = a;
   return GGB_OK;
+}
+
+int ggb_sa_create_symmetric(int nodes, int degree, int groups, const int* edges, int candidates, int compose_max,
+                            unsigned long long seed, ggb_sa** out) {
+  if (groups == 1) return ggb_sa_create(nodes, degree, edges, candidates, candidates, compose_max, seed, out);
+  if (!out || !edges) return core_fail(GGB_EINVAL, "null pointer");
+  *out = nullptr;
+  if (groups < 2 || nodes % groups || nodes / groups < 3)
+    return core_fail(GGB_EINVAL, "groups must divide nodes, with at least 3 vertices per group");
+  if (nodes < 4 || degree < 1 || ((long long)nodes * degree) % (2LL * groups) || (long long)nodes * degree > INT_MAX)
+    return core_fail(GGB_EINVAL, "nodes*degree must be a multiple of 2*groups");
+  if (candidates < 1 || candidates > ggb::sa::kComposeThreads)
+    return core_fail(GGB_EINVAL, "candidates must be in [1, %d]", ggb::sa::kComposeThreads);
+  if (compose_max < 0 || compose_max > 4096) return core_fail(GGB_EINVAL, "compose_max must be in [0, 4096]");
+  ggb_sa* a = new ggb_sa();
+  int rc = create(a, nodes, degree, groups, edges, candidates, candidates, compose_max, seed);
+  if (rc) {
+    destroy(a);
+    return rc;
+  }
+  *out = a;
+  return GGB_OK;
+}
+
+int ggb_sa_set_grid(ggb_sa* a, int height, int max_length) {
+  if (!a) return core_fail(GGB_EINVAL, "null annealer");
+  if (a->groups != 1) return core_fail(GGB_EPERM, "grid length limits are served for graphs without symmetry");
+  if (height < 1 || a->N % height || max_length < 1)
+    return core_fail(GGB_EINVAL, "height must divide nodes and max_length must be >= 1");
+  SCUDA(cudaSetDevice(a->device));
+  SCUDA(cudaStreamSynchronize(a->st));
+  std::vector<int> e((size_t)2 * a->lines);
+  SCUDA(cudaMemcpy(e.data(), a->d_edges, e.size() * sizeof(int), cudaMemcpyDeviceToHost));
+  for (int l = 0; l < a->lines; ++l) {
+    const int u = e[2 * l], v = e[2 * l + 1];
+    const int len = std::abs(u / height - v / height) + std::abs(u % height - v % height);
+    if (len > max_length)
+      return core_fail(GGB_EINVAL, "line %d (%d, %d) is longer than %d on the lattice", l, u, v, max_length);
+  }
+  int rc = pull_state(a);
+  if (rc) return rc;
+  a->h.grid_height = height;
+  a->h.grid_length = max_length;
+  return push_state(a);
 }
 
 void ggb_sa_destroy(ggb_sa* a) { destroy(a); }
@@ -1281,8 +1519,8 @@ int ggb_sa_set_predicted(ggb_sa* a, int composites, int max_swaps) {
   if (rc) return rc;
   if (a->compose_max >= 2 || a->C > 0) {
     const int nc = 1 + a->C;
-    std::vector<int> nn(nc, a->N), gg(nc, 1), dd(nc, a->d);
-    if ((rc = ggb_batch_create(nc, nn.data(), nn.data(), gg.data(), dd.data(), &a->comp))) return rc;
+    std::vector<int> nn(nc, a->N), bn(nc, a->N / a->groups), gg(nc, a->groups), dd(nc, a->d);
+    if ((rc = ggb_batch_create(nc, nn.data(), bn.data(), gg.data(), dd.data(), &a->comp))) return rc;
     a->comp->stop = &a->d_state->done;
     a->comp->sticky = a->d_sticky;
     for (int k = 0; k < nc; ++k) {
@@ -1331,6 +1569,7 @@ int ggb_sa_run(ggb_sa* a, long long steps, ggb_sa_stats* stats) {
   if (rc) return rc;
   rc = pull_state(a);
   if (rc) return rc;
+  if (a->h.move_error) return core_fail(GGB_ECUDA, "an accepted move did not match the current graph");
   if (stats) {
     const double pairs = (double)a->N * (a->N - 1);
     stats->step = a->h.step;

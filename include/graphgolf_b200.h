@@ -351,6 +351,23 @@ typedef struct ggb_sa_stats {
  * 16 up to 4096 (then candidates is a multiple of 16, degree <= 32). */
 int ggb_sa_create(int nodes, int degree, const int *edges, int candidates, int proposals, int compose_max,
                   unsigned long long seed, ggb_sa **out);
+/* The same for a graph with `groups` rotational symmetry groups (invariant
+ * under v -> v + nodes/groups, edges in the reference's symmetric line order:
+ * line k*BL + i is line i shifted by k*nodes/groups, general/main.c:175-183).
+ * Every move keeps the symmetry: two random lines of different orbits are
+ * swapped in every copy (2g-opt, general/sa.c:217-369), two lines of one orbit
+ * re-pair that orbit with a random shift (1g-opt, general/common.c:162-276);
+ * the four endpoint classes (v mod nodes/groups) must be distinct.  Each
+ * candidate is evaluated in full over nodes/groups sources and Metropolis uses
+ * the reference's diff = change of the distance total / groups.  No proposal
+ * filter (candidates = proposals); groups = 1 is ggb_sa_create. */
+int ggb_sa_create_symmetric(int nodes, int degree, int groups, const int *edges, int candidates, int compose_max,
+                            unsigned long long seed, ggb_sa **out);
+/* Grid graphs without symmetry (grid/sa.c:137-221): vertex v is lattice
+ * point (v / height, v % height) and every move keeps both new edges within
+ * Manhattan length max_length.  Every current edge must already be within
+ * it.  Set before running. */
+int ggb_sa_set_grid(ggb_sa *a, int height, int max_length);
 void ggb_sa_destroy(ggb_sa *a);
 /* Temperature, cooling factor per step, and hill climbing (the reference's
  * -H: accept only when not worse).  Default: hill climbing. */

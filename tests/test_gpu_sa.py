@@ -211,3 +211,91 @@ def test_filter_beats_random_selection(gpu):
         assert np.mean(top < 0) > 1.5 * np.mean(rnd < 0)
         assert top.mean() < rnd.mean()
         _check(an, g, an.run(0))
+
+
+def _check_symmetric(an, g, st):
+    """Both reported states are exact, and the edges the device holds are
+    simple, regular and in the symmetric line order (line k*BL + i is line i
+    shifted by k*B), so the graph really has the symmetry its group-weighted
+    evaluation assumes: the oracle's full evaluation (every source) agrees."""
+    B, n = g.nodes // g.groups, g.nodes
+    for best, want in ((False, (st.cur_diam, st.cur_total)), (True, (st.best_diam, st.best_total))):
+        e = an.edges(best=best)
+        BL = e.shape[0] // g.groups
+        for k in range(1, g.groups):
+            assert np.array_equal(e[k * BL:(k + 1) * BL], (e[:BL] + k * B) % n)
+        adj = graphs.create_adj(n, g.degree, e)
+        assert graphs.verify(graphs.Graph(n, g.degree, e, adj)) == 0
+        _, diam, _, total = oracle.general(adj, groups=g.groups)
+        assert (diam, total) == want
+        assert oracle.general(adj)[1::2] == (diam, total)
+
+
+@pytest.mark.parametrize("n,d,grp,K,comp", [(2048, 8, 4, 1, 0), (2048, 8, 16, 16, 8), (1500, 6, 3, 8, 4),
+                                            (4096, 12, 2, 32, 16)])
+def test_symmetric_states_exact(gpu, n, d, grp, K, comp):
+    """Orbit moves (2g-opt and 1g-opt) keep the graph symmetric; candidates are
+    evaluated over n/groups sources, every state equals the oracle's."""
+    g = graphs.symmetric_regular(n, d, grp, 30 + grp)
+    with gg.Annealer(g, candidates=K, compose=comp, seed=9) as an:
+        st0 = an.run(0)
+        _, diam, _, total = oracle.general(g.adj, groups=grp)
+        assert (st0.cur_diam, st0.cur_total) == (diam, total)
+        prev = st0.cur_total
+        for _ in range(3):
+            st = an.run(15)
+            assert st.cur_total <= prev
+            prev = st.cur_total
+            _check_symmetric(an, g, st)
+        assert st.accepts > 0 and not st.delta
+        assert st.cur_total < st0.cur_total
+
+
+def test_symmetric_metropolis_states_exact(gpu):
+    g = graphs.symmetric_regular(1024, 6, 8, 3)
+    with gg.Annealer(g, candidates=4, seed=2) as an:
+        an.schedule(50.0, 0.98, hill_climbing=False)
+        for _ in range(3):
+            st = an.run(20)
+            _check_symmetric(an, g, st)
+
+
+@pytest.mark.parametrize("K,G,comp", [(1, 1, 0), (32, 32, 8), (32, 256, 16)])
+def test_grid_states_exact(gpu, K, G, comp):
+    """Grid graphs: every move keeps both new edges within the length limit
+    (grid/sa.c:137-221); every state equals the oracle's grid evaluation,
+    plain, batched (delta path) and with the proposal filter."""
+    w = h = 30
+    g = graphs.grid_regular(w, h, 4, 3, 7)
+    rh = graphs.rotate_hash(g.nodes, h, w, 1)
+    with gg.Annealer(g, candidates=K, proposals=G, compose=comp, seed=5) as an:
+        an.grid(h, 3)
+        st0 = an.run(0)
+        prev = st0.cur_total
+        for _ in range(3):
+            st = an.run(10)
+            assert st.cur_total <= prev
+            prev = st.cur_total
+            for best, want in ((False, (st.cur_diam, st.cur_total)), (True, (st.best_diam, st.best_total))):
+                e = an.edges(best=best)
+                adj = graphs.create_adj(g.nodes, 4, e)
+                assert graphs.verify(graphs.Graph(g.nodes, 4, e, adj, width=w, height=h), max_len=3) == 0
+                ok, diam, _, total = oracle.grid(adj, rh)
+                assert ok and (diam, total) == want
+        assert st.cur_total < st0.cur_total
+
+
+def test_orbit_and_grid_inputs_rejected(gpu):
+    g = graphs.symmetric_regular(512, 6, 4, 1)
+    bad = graphs.Graph(g.nodes, g.degree, g.edges[::-1].copy(), g.adj, groups=4)
+    with pytest.raises(gg.EvaluationError):
+        gg.Annealer(bad, candidates=4)
+    with pytest.raises(ValueError):
+        gg.Annealer(g, candidates=16, proposals=64)
+    with gg.Annealer(g, candidates=4) as an:
+        with pytest.raises(gg.EvaluationError):
+            an.grid(16, 3)   # no length limits on symmetric graphs
+    gr = graphs.grid_regular(20, 20, 4, 3, 2)
+    with gg.Annealer(gr, candidates=4) as an:
+        with pytest.raises(gg.EvaluationError):
+            an.grid(20, 1)   # the current graph already has longer edges
