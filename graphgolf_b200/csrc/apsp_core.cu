@@ -116,6 +116,7 @@ struct State {
   long long timeout_ns = 2000000000LL;
   int phantom = 0;
   uint4* d_ball = nullptr;    size_t cap_ball = 0;    // uint4, ball pre-pass matrix
+  unsigned* d_stamps = nullptr; size_t cap_stamps = 0; // full-row stamps, one per vertex
   unsigned long long* d_ball_cnt = nullptr; size_t cap_ball_cnt = 0;
   int ball_mode = -1;         // -1 automatic, 0 never, 1 whenever feasible
   int ball_occ = 0;           // co-resident ball CTAs per SM at the last size
@@ -355,6 +356,14 @@ int launch_apsp(const int* d_adj, int N, int d, int n_src1, int split, int ac, i
   a.ball = use_ball ? g.d_ball : nullptr;
   a.ball_cnt = use_ball ? g.d_ball_cnt : nullptr;
   a.win_bits = W < 128 * R ? W : 0;
+  if (const char* sp = getenv("GGB_SKIP_PERMILLE")) a.skip_permille = atoi(sp);
+  // full-row stamps: the skipping sweep of 4096-bit rows, degree <= 16
+  if (R == 32 && d <= 16 && W == 128 * R) {
+    rc = grow_device(&g.d_stamps, &g.cap_stamps, (size_t)N);
+    if (rc) return rc;
+    CUDA_TRY(cudaMemsetAsync(g.d_stamps, 0, (size_t)N * sizeof(unsigned), st));
+    a.stamps = g.d_stamps;
+  }
   CUDA_TRY(cudaMemsetAsync(g.d_ctrl, 0, sizeof(ApspCtrl), st));
   if (g.timing) CUDA_TRY(cudaEventRecord(g.ev[0], st));
   if (use_ball) {
@@ -533,6 +542,7 @@ void ggb_finalize(void) {
     if (e) cudaEventDestroy(e);
   cudaFree(g.d_ball);
   cudaFree(g.d_ball_cnt);
+  cudaFree(g.d_stamps);
   cudaFreeHost(g.h_adj);
   cudaFreeHost(g.h_rh);
   cudaFreeHost(g.h_ctrl);

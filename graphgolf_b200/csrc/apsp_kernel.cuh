@@ -104,6 +104,14 @@ struct ApspArgs {
   // (the reference's one-word chunk, general/evaluation.cu:27-44) on rows of
   // one uint4 whose upper 64 bits stay zero.  0: W = 128 * R.
   int win_bits = 0;
+  // The skipping sweep runs once the gathered level is at least this full
+  // (per mille of N * sources).
+  int skip_permille = 900;
+  // Optional full-row stamps, one per vertex, zeroed before the launch
+  // (single-graph evaluations only): stamp = (window id << 8) | L records that
+  // the vertex's row of that window is full from level L on.  The sweeps that
+  // set and read them are described at sweep_stamped.
+  unsigned* stamps = nullptr;
 };
 
 __device__ __forceinline__ unsigned long long globaltimer_ns() {
@@ -790,6 +798,110 @@ __device__ __forceinline__ void sweep_wide_half(const uint4* __restrict__ src, u
   }
 }
 
+// Full-row stamps.  A row that is full at level L stays full (the sets are
+// monotone), so its later rows need neither a read nor a write: the plain
+// sweep stamps every row it finds full, and the stamped sweep below -- the
+// skipping sweep of 4096-bit rows, degree <= 16 -- counts a stamped row as
+// full without touching it, treats a row with a stamped neighbour as full
+// (S_{k+1}[v] contains S_k[u]), and stamps instead of writing every row that
+// turns full.  Its readers are therefore all stamp-aware: a row is read only
+// when its stamp says it is not full, and such a row was written by the sweep
+// that produced it.  The skipping sweeps are the last sweeps of a window (its
+// levels only fill up), so no plain sweep ever reads a row left unwritten.
+__device__ __forceinline__ bool stamped_full(unsigned st, unsigned id, int k) {
+  return (st >> 8) == id && (int)(st & 0xffu) <= k;
+}
+
+template <int R>
+__device__ __forceinline__ void sweep_stamped(const uint4* __restrict__ src, uint4* __restrict__ dst,
+                                              const int* __restrict__ adj, int N, int d, int split, long long warp_id,
+                                              long long n_warps, int l, unsigned (&cl)[4], bool& adj_ok,
+                                              unsigned* __restrict__ stamps, unsigned id, int k) {
+  static_assert(R == 32, "two uint4 of the row a lane");
+  constexpr int U = 4;
+  const int lane = threadIdx.x & 31, h = lane >> 4, hl = lane & 15;
+  const uint4 zero = make_uint4(0u, 0u, 0u, 0u);
+  const uint4 fm[2] = {chunk_full_mask(2 * hl, l), chunk_full_mask(2 * hl + 1, l)};
+  auto full = [&](const uint4 (&r)[2]) { return equal4(r[0], fm[0]) && equal4(r[1], fm[1]); };
+  const unsigned new_stamp = (id << 8) | (unsigned)(k + 1);
+  const bool can_stamp = k + 1 < 255;
+  // a contiguous block of vertices per warp: one coalesced stamp load per 32
+  const long long per = ((long long)N + n_warps - 1) / n_warps;
+  const long long v_lo = warp_id * per, v_hi = min((long long)N, v_lo + per);
+  for (long long b = v_lo; b < v_hi; b += 32) {
+    const long long v = b + lane;
+    const bool in = v < v_hi;
+    const bool fl = in && stamped_full(__ldcg(stamps + v), id, k);
+    const unsigned fullm = __ballot_sync(0xffffffffu, fl);
+    unsigned todo = __ballot_sync(0xffffffffu, in) & ~fullm;
+    if (lane == 0 && fullm) {
+      // full rows count l each, lo rows (v < split) and hi rows apart
+      const long long lo_n = split - b;
+      const unsigned lo_m = lo_n >= 32 ? 0xffffffffu : (lo_n <= 0 ? 0u : ((1u << lo_n) - 1u));
+      cl[0] += (unsigned)__popc(fullm & lo_m) * (unsigned)l;
+      cl[1] += (unsigned)__popc(fullm & ~lo_m) * (unsigned)l;
+    }
+    while (todo) {   // warp-uniform: two vertices per step, one per half-warp
+      const int i0 = __ffs(todo) - 1;
+      todo &= todo - 1;
+      int i1 = -1;
+      if (todo) {
+        i1 = __ffs(todo) - 1;
+        todo &= todo - 1;
+      }
+      const int my = h == 0 ? i0 : i1;
+      const bool live = my >= 0;
+      const long long vv = b + (live ? my : 0);
+      int u = 0;
+      bool nfull = false;
+      if (live && hl < d) {
+        u = __ldg(adj + vv * d + hl);
+        if ((unsigned)u >= (unsigned)N) { adj_ok = false; u = 0; }
+        nfull = stamped_full(__ldcg(stamps + u), id, k);
+      }
+      const unsigned nb = __ballot_sync(0xffffffffu, nfull);
+      const bool any_nfull = ((nb >> (h << 4)) & 0xffffu) != 0u;
+      uint4 acc[2] = {fm[0], fm[1]};
+      if (live && !any_nfull) ld_cg2(src + vv * R + 2 * hl, acc);
+      bool need = live && !any_nfull && !full(acc);
+      for (int j0 = 0; j0 < d; j0 += U) {
+        uint4 x[U][2];
+#pragma unroll
+        for (int q = 0; q < U; ++q) {
+          const int j = j0 + q;
+          const int uj = __shfl_sync(0xffffffffu, u, (h << 4) | (j & 15));
+          if (j < d && need) {
+            ld_cg2(src + (long long)uj * R + 2 * hl, x[q]);
+          } else {
+            x[q][0] = zero;
+            x[q][1] = zero;
+          }
+        }
+#pragma unroll
+        for (int q = 0; q < U; ++q) {
+          or_into(acc[0], x[q][0]);
+          or_into(acc[1], x[q][1]);
+        }
+        need = need && !full(acc);
+      }
+      const unsigned fb = __ballot_sync(0xffffffffu, full(acc));
+      const bool row_full = ((fb >> (h << 4)) & 0xffffu) == 0xffffu;
+      if (live) {
+        if (row_full && can_stamp) {
+          if (hl == 0) {
+            stamps[vv] = new_stamp;
+            if (vv < split) cl[0] += (unsigned)l; else cl[1] += (unsigned)l;
+          }
+        } else {
+          st_cg2(dst + vv * R + 2 * hl, acc);
+          const unsigned cc = popc4(acc[0]) + popc4(acc[1]);
+          if (vv < split) cl[0] += cc; else cl[1] += cc;
+        }
+      }
+    }
+  }
+}
+
 // ---- one graph on a team of CTAs ------------------------------------------------
 // R = uint4 words per row (W = 128*R source bits).  LPR lanes share a row,
 // each lane owning UPL uint4 of it; a warp covers VPW vertices per step.
@@ -876,6 +988,9 @@ __device__ __forceinline__ bool eval_windows(const ApspArgs& a, int cta, int nct
       const uint4* cur;           // S_kk rows the next sweep gathers from
       uint4* nxt;                 // rows it writes
       bool own_count = false;     // the first sweep of a ball window also reports S_3
+      // full-row stamps: phase-1 windows of single-graph evaluations, id = t + 1
+      unsigned* const stamps = (phase == 1 && a.levels == nullptr && !STATS) ? a.stamps : nullptr;
+      const unsigned stamp_id = (unsigned)t + 1u;
       // base builds: this window's level rows and counts (never with the ball pre-pass)
       uint4* const lev0 = a.levels ? a.levels + (size_t)t * (a.level_cap + 1) * N * R : nullptr;
       long long* const lcnt = a.levels ? a.level_counts + (size_t)t * (a.level_cap + 1) : nullptr;
@@ -943,14 +1058,18 @@ __device__ __forceinline__ bool eval_windows(const ApspArgs& a, int cta, int nct
           // plain sweep is faster.
           bool wide = false;
           if constexpr (LPR == 32) {
-            if (d <= 32 && !own_count && prev_total * 10 >= (long long)N * l * 9) {
+            if (d <= 32 && !own_count && prev_total * 1000 >= (long long)N * l * a.skip_permille) {
               wide = true;
               bool half = false;
               if constexpr (R == 32) {
                 if (d <= 16) {
                   half = true;
-                  sweep_wide_half<R, STATS>(src, dst, adjp, N, d, a.split, slot, n_slots, l, cl, adj_ok, a.stats,
-                                            (int)kk + 1);
+                  if (!STATS && stamps)
+                    sweep_stamped<R>(src, dst, adjp, N, d, a.split, warp_id, n_warps, l, cl, adj_ok, stamps,
+                                     stamp_id, (int)kk);
+                  else
+                    sweep_wide_half<R, STATS>(src, dst, adjp, N, d, a.split, slot, n_slots, l, cl, adj_ok,
+                                              a.stats, (int)kk + 1);
                 }
               }
               if (!half)
@@ -1023,11 +1142,27 @@ __device__ __forceinline__ bool eval_windows(const ApspArgs& a, int cta, int nct
                 }
                 if (v < a.split) cl[0] += cc; else cl[1] += cc;
               }
-              if constexpr (STATS) {
-                // the LP lanes of this row hold its popcount in parts
-                unsigned tot = cc;
+              if constexpr (R == 32) {
+                // (one row pair per warp step at R = 32, so the loop is warp-uniform); rows
+                // turn full only once the gathered level is well filled: below 30 % of
+                // N * sources nothing is stamped
+                if (stamps && d <= 16 && prev_total * 10 >= (long long)N * l * 3) {
+                  // the LP lanes of this row hold its popcount in parts
+                  unsigned tot = cc;
 #pragma unroll
-                for (int o = LP / 2; o > 0; o >>= 1) tot += __shfl_xor_sync(0xffffffffu, tot, o);
+                  for (int o = LP / 2; o > 0; o >>= 1) tot += __shfl_xor_sync(0xffffffffu, tot, o);
+                  if (live && hl == 0 && tot == (unsigned)l && kk + 1 < 255)
+                    stamps[v] = (stamp_id << 8) | (unsigned)(kk + 1);
+                }
+              }
+              if constexpr (STATS) {
+                // the LP lanes of this row hold its popcount in parts; with several rows a
+                // warp step (R < 32) the groups may leave the loop apart, so only the lanes
+                // still in it take part
+                unsigned tot = cc;
+                const unsigned am = __activemask();
+#pragma unroll
+                for (int o = LP / 2; o > 0; o >>= 1) tot += __shfl_xor_sync(am, tot, o);
                 if (live && hl == 0 && kk + 1 < kStatLevels)
                   atomicAdd(a.stats + v * kStatLevels + kk + 1, (unsigned)l - tot);
               }
