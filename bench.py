@@ -398,6 +398,9 @@ def main() -> int:
     ap.add_argument("--no-ref-gpu", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the mixed-batch measurement")
     ap.add_argument("--no-sa", action="store_true", help="skip the annealing race")
+    ap.add_argument("--shard", action="store_true",
+                    help="one graph per job, its source windows spread over the ranks (the reference's MPI "
+                         "split) with a 16-byte NCCL all-reduce: strong scaling")
     ap.add_argument("--no-widths", action="store_true",
                     help="skip the window-width sweep (64..512 bits) and the g=16 symmetric graph")
     ap.add_argument("--sa-plain-steps", type=int, default=30000, help="plain annealing steps that set the target")
@@ -433,6 +436,8 @@ def main() -> int:
     lib = gg.load()
     if lib.ggb_init(local, wl["nodes"], wl["degree"]) != 0:
         raise RuntimeError(_native.last_error())
+    if args.shard:
+        return run_sharded(args, wl, lib, rank, world, local, dist)
     if args.window_bits:
         gg.set_tuning(args.window_bits, 0)
     gg.set_ball(args.ball)
@@ -556,6 +561,82 @@ def main() -> int:
         line["batch"] = batch_bench(peak, peak_kind, lib)
     if rank == 0 and world == 1 and not args.no_sa:
         line["sa"] = sa_bench(args.sa_plain_steps)
+    if rank == 0:
+        print(json.dumps(line))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def run_sharded(args, wl, lib, rank: int, world: int, local: int, dist) -> int:
+    """One evaluation of the bench graph per step with its source windows
+    spread over the ranks: rank r runs windows r, r + world, ... (the
+    reference's MPI split, general/evaluation.c:166) and the ranks join
+    diameter and distance sum with two all-reduces of 8 and 16 bytes (NCCL;
+    general/evaluation.c:247-248).  Time per step: CUDA events on the
+    launching stream around the partial evaluation, the read-back and the
+    all-reduces; max over ranks.  value = evaluations per second of the job
+    (strong scaling: the graph does not grow with the ranks)."""
+    import numpy as np
+    import torch
+    import graphgolf_b200 as gg
+    from graphgolf_b200 import _native
+    from graphgolf_b200.distributed import allreduce_partial
+    n, d, groups = wl["nodes"], wl["degree"], wl["groups"]
+    g = _graph(wl, 0)                       # the same graph on every rank
+    adj_dev = torch.from_numpy(np.ascontiguousarray(g.adj)).cuda()
+    stream = torch.cuda.Stream()
+    sptr = C.c_void_p(stream.cuda_stream)
+    flush = torch.empty(max(args.flush_mib, 200) * 1024 * 1024, dtype=torch.uint8, device="cuda")
+    part = _native.ggb_partial()
+
+    def step(ev=None):
+        with torch.cuda.stream(stream):
+            flush.fill_(1)
+            if ev:
+                ev[0].record(stream)
+            if lib.ggb_launch_general_partial_device(n, n // groups, groups, d, adj_dev.data_ptr(), 0, rank, world,
+                                                     sptr):
+                raise RuntimeError(_native.last_error())
+            if lib.ggb_collect_partial(sptr, C.byref(part)):
+                raise RuntimeError(_native.last_error())
+            if dist:
+                diam, disc, total = allreduce_partial(part, device="cuda")
+            else:
+                diam, disc, total = part.diam, part.disconnected, part.sum
+            if ev:
+                ev[1].record(stream)
+        return gg.finish_general(n, diam, disc, total)
+
+    for _ in range(args.warmup):
+        first = step()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with Clocks(local) as clk:
+        for k in range(args.steps):
+            r = step(evs[k])
+            assert (r.diameter, r.total) == (first.diameter, first.total)
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    t = sum(a.elapsed_time(b) for a, b in evs) / 1e3
+    t_max = t
+    if dist:
+        tt = torch.tensor([t], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_max = float(tt.item())
+    line = {"metric": METRIC, "value": args.steps / t_max, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_max / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "u64",
+            "data": "synthetic (seeded random regular graph, per-pair-retry pairing model)",
+            "config": {**common_config(args, wl),
+                       "parallelism": f"source windows of one graph over {world} ranks, 16-byte all-reduce"},
+            "run": {"diameter": first.diameter, "total": first.total, "windows_per_rank": part.windows,
+                    "window_bits": part.window_bits},
+            "gpu_launches": None, "clocks": clk.summary()}
     if rank == 0:
         print(json.dumps(line))
     if dist:

@@ -92,6 +92,8 @@ CORE_SIGNATURES = {
     "ggb_eval_general_device": (_I, [_I, _I, _I, _I, _P, _I, _P, C.POINTER(ggb_result)]),
     "ggb_launch_general_device": (_I, [_I, _I, _I, _I, _P, _I, _P]),
     "ggb_collect": (_I, [_P, C.POINTER(ggb_result)]),
+    "ggb_launch_general_partial_device": (_I, [_I, _I, _I, _I, _P, _I, _I, _I, _P]),
+    "ggb_collect_partial": (_I, [_P, C.POINTER(ggb_partial)]),
     "ggb_kernel_launches": (_LL, []),
     "ggb_trace_enable": (_I, [_I]),
     "ggb_set_timing": (_I, [_I]),

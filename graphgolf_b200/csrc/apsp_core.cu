@@ -723,6 +723,27 @@ int ggb_launch_general_device(int nodes, int based_nodes, int groups, int degree
                      1, pick_stream(stream));
 }
 
+int ggb_launch_general_partial_device(int nodes, int based_nodes, int groups, int degree, const int* adj_dev,
+                                      int added_centers, int rank, int procs, void* stream) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (!adj_dev && nodes * degree) return fail(GGB_EINVAL, "null adjacency");
+  if (procs <= 0 || rank < 0 || rank >= procs) return fail(GGB_EINVAL, "rank %d of %d", rank, procs);
+  int rc = check_general(nodes, based_nodes, groups, degree, added_centers);
+  if (rc) return rc;
+  rc = ensure_ready(-1);
+  if (rc) return rc;
+  g.last_grid = false;
+  return launch_apsp(adj_dev, nodes, degree, based_nodes, based_nodes * groups, added_centers, groups, rank,
+                     procs, pick_stream(stream));
+}
+
+int ggb_collect_partial(void* stream, ggb_partial* out) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (!out) return fail(GGB_EINVAL, "null pointer");
+  if (!g.ready) return fail(GGB_EINVAL, "nothing launched");
+  return read_ctrl(pick_stream(stream), out);
+}
+
 int ggb_collect(void* stream, ggb_result* out) {
   std::lock_guard<std::mutex> lk(g_mu);
   if (!out) return fail(GGB_EINVAL, "null pointer");

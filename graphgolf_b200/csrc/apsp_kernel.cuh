@@ -1101,6 +1101,12 @@ __device__ __forceinline__ bool eval_windows(const ApspArgs& a, int cta, int nct
                 if (v < a.split) cl[2] += co; else cl[3] += co;
               }
               int j = 0;
+              // After a group of neighbour rows, a part of the row whose 256
+              // bits are all set needs no further gathers (full-width windows
+              // only: every bit of the part is a source).
+              bool need[PPL];
+#pragma unroll
+              for (int p = 0; p < PPL; ++p) need[p] = true;
               for (; j + U2 <= d; j += U2) {
                 int u[U2];
 #pragma unroll
@@ -1109,11 +1115,24 @@ __device__ __forceinline__ bool eval_windows(const ApspArgs& a, int cta, int nct
                 for (int q = 0; q < U2; ++q) {
                   if ((unsigned)u[q] >= (unsigned)N) { adj_ok = false; u[q] = 0; }
                 }
+                if (j > 0 && l == W) {
+#pragma unroll
+                  for (int p = 0; p < PPL; ++p)
+                    need[p] = (acc[p][0].x & acc[p][0].y & acc[p][0].z & acc[p][0].w & acc[p][1].x & acc[p][1].y &
+                               acc[p][1].z & acc[p][1].w) != 0xffffffffu;
+                }
                 uint4 x[U2][PPL][2];
 #pragma unroll
                 for (int q = 0; q < U2; ++q)
 #pragma unroll
-                  for (int p = 0; p < PPL; ++p) ld_cg2(src + (long long)u[q] * R + 2 * (hl + p * LP), x[q][p]);
+                  for (int p = 0; p < PPL; ++p) {
+                    if (need[p]) {
+                      ld_cg2(src + (long long)u[q] * R + 2 * (hl + p * LP), x[q][p]);
+                    } else {
+                      x[q][p][0] = make_uint4(0u, 0u, 0u, 0u);
+                      x[q][p][1] = make_uint4(0u, 0u, 0u, 0u);
+                    }
+                  }
 #pragma unroll
                 for (int q = 0; q < U2; ++q)
 #pragma unroll

@@ -15,10 +15,21 @@
  * range, invalid sizes) prints a message and aborts the process, as the
  * reference's ERROR() does (general/common.h:67-70): returning false there
  * would make sa.c propose moves forever (general/sa.c:452-479).
+ *
+ * MPI hosts: built with -DGGB_WITH_MPI against the host's <mpi.h> (the
+ * reference builds with mpicc, general/Makefile:1-8), a run with procs > 1
+ * splits every evaluation as the reference's own evaluation() does: rank r
+ * evaluates source windows r, r + procs, ... on its GPU (rank % gpus, as
+ * init_matrix_dev picks it) and the ranks join diameter and distance sum with
+ * two MPI_Allreduce calls (general/evaluation.c:166,247-248).  Without
+ * -DGGB_WITH_MPI every rank evaluates the whole graph.
  */
 #include <stdbool.h>
 #include <stdio.h>
 #include <stdlib.h>
+#ifdef GGB_WITH_MPI
+#include <mpi.h>
+#endif
 
 #define GGB_DROPIN_GENERAL
 #include "../../include/graphgolf_b200.h"
@@ -28,6 +39,7 @@
 extern void timer_start(const int n) __attribute__((weak));
 extern void timer_stop(const int n) __attribute__((weak));
 extern int rank __attribute__((weak));
+extern int procs __attribute__((weak));
 
 #define GGB_TIMER_APSP 2 /* general/common.h:41 */
 
@@ -59,7 +71,33 @@ bool evaluation(const int nodes, const int based_nodes, const int groups, const 
   (void)algo;
   if (timer_start) timer_start(GGB_TIMER_APSP);
   ggb_result r;
-  int rc = ggb_eval_general(nodes, based_nodes, groups, degree, adj, added_centers, &r);
+  int rc;
+#ifdef GGB_WITH_MPI
+  if (&procs != NULL && &rank != NULL && procs > 1) {
+    ggb_partial p;
+    rc = ggb_eval_general_partial(nodes, based_nodes, groups, degree, adj, added_centers, rank, procs, &p);
+    if (rc) die("evaluation", rc);
+    /* MAX of (diameter, disconnected, window width, -window width): every rank
+     * must have cut the sources into the same windows */
+    int mx[4] = {p.diam, p.disconnected, p.window_bits, -p.window_bits};
+    long long sm = p.sum;
+    MPI_Allreduce(MPI_IN_PLACE, mx, 4, MPI_INT, MPI_MAX, MPI_COMM_WORLD);
+    MPI_Allreduce(MPI_IN_PLACE, &sm, 1, MPI_LONG_LONG, MPI_SUM, MPI_COMM_WORLD);
+    if (mx[2] != -mx[3]) {
+      fprintf(stdout, "graphgolf_b200: ranks cut the sources into different windows (%d and %d bits)\n", mx[2],
+              -mx[3]);
+      fflush(stdout);
+      abort();
+    }
+    p.diam = mx[0];
+    p.disconnected = mx[1];
+    p.sum = sm;
+    rc = ggb_finish_general(nodes, &p, &r);
+  } else
+#endif
+  {
+    rc = ggb_eval_general(nodes, based_nodes, groups, degree, adj, added_centers, &r);
+  }
   if (rc) die("evaluation", rc);
   *diameter = r.diameter;
   *ASPL = r.aspl;

@@ -226,6 +226,13 @@ const char *ggb_noalloc_last_error(void);
 int ggb_eval_general_partial(int nodes, int based_nodes, int groups, int degree, const int *adj,
                              int added_centers, int rank, int procs, ggb_partial *out);
 
+/* Device-resident form of ggb_eval_general_partial: enqueues rank's share
+ * on `stream` without waiting; ggb_collect_partial waits and returns it.
+ * Used to time the sharded evaluation (bench.py --shard). */
+int ggb_launch_general_partial_device(int nodes, int based_nodes, int groups, int degree, const int *adj_dev,
+                                      int added_centers, int rank, int procs, void *stream);
+int ggb_collect_partial(void *stream, ggb_partial *out);
+
 /* Completes reduced partials into the general convention
  * (general/evaluation.c:247-262). */
 int ggb_finish_general(int nodes, const ggb_partial *reduced, ggb_result *out);

@@ -79,19 +79,48 @@ def test_small_config_full_sa_identical(gpu, tmp_path):
 
 def test_grid_config_prefix_identical(gpu, tmp_path):
     """The grid configuration at its size: a 100 x 100 lattice, degree 4,
-    edge length limit 3, the first 300 annealing steps (the host-side
-    reference needs about 0.02-0.2 s per evaluation at this size, so the
-    full 100 000 steps are out of reach of a test), reference OpenMP
-    evaluator against this repository's."""
+    edge length limit 3, the first 2 000 annealing steps, reference OpenMP
+    evaluator against this repository's, run side by side."""
     _need("gg_grid_openmp", "gg_grid_b200")
     gr = graphs.grid_regular(100, 100, 4, 3, 1)
     f = tmp_path / "in.edges"
     graphs.write_grid(str(f), gr)
-    args = ["-f", str(f), "-R", "3", "-s", "1", "-n", "300"]
+    args = ["-f", str(f), "-R", "3", "-s", "1", "-n", "2000"]
     cpu = _run("gg_grid_openmp", args + ["-o", str(tmp_path / "cpu.edges")], tmp_path)
     gpu_out = _run("gg_grid_b200", args + ["-o", str(tmp_path / "gpu.edges")], tmp_path)
     assert _stable(cpu) == _stable(gpu_out)
     assert (tmp_path / "cpu.edges").read_text() == (tmp_path / "gpu.edges").read_text()
+
+
+def test_grid_config_full_trajectory_identical(gpu, tmp_path):
+    """The whole grid configuration: 100 000 annealing steps of the reference's
+    own grid program linked against libgg_grid.so must reproduce, row for
+    row, the progress table and the final graph of the same program run once
+    on the CPU with the reference's own evaluator
+    (tests/golden/grid_trajectory_w100h100d4r3.json, made by
+    tests/golden/make_grid_trajectory.py)."""
+    import hashlib
+    import json
+    import sys
+    gold = Path(__file__).resolve().parent / "golden"
+    fx = gold / "grid_trajectory_w100h100d4r3.json"
+    if not fx.exists():
+        pytest.skip("the grid trajectory fixture has not been generated")
+    _need("gg_grid_b200")
+    sys.path.insert(0, str(gold))
+    from make_grid_trajectory import program_args, stable_lines, write_input
+    want = json.loads(fx.read_text())
+    fin, fout = tmp_path / "in.edges", tmp_path / "out.edges"
+    write_input(str(fin))
+    assert hashlib.sha256(fin.read_bytes()).hexdigest() == want["input_sha256"], "generator drift"
+    p = subprocess.run([str(REF / "gg_grid_b200"), *program_args(str(fin), str(fout))], cwd=tmp_path,
+                       capture_output=True, text=True, timeout=1800)
+    assert p.returncode == 0, p.stdout[-2000:] + p.stderr[-2000:]
+    got = stable_lines(p.stdout)
+    for i, (a, b) in enumerate(zip(got, want["lines"])):
+        assert a == b, f"first difference at line {i}: {a!r} != {b!r}"
+    assert len(got) == len(want["lines"])
+    assert hashlib.sha256(fout.read_bytes()).hexdigest() == want["output_sha256"]
 
 
 def test_general_startup_randomisation_identical(gpu, tmp_path):
