@@ -356,7 +356,6 @@ int launch_apsp(const int* d_adj, int N, int d, int n_src1, int split, int ac, i
   a.ball = use_ball ? g.d_ball : nullptr;
   a.ball_cnt = use_ball ? g.d_ball_cnt : nullptr;
   a.win_bits = W < 128 * R ? W : 0;
-  if (const char* sp = getenv("GGB_SKIP_PERMILLE")) a.skip_permille = atoi(sp);
   // full-row stamps: the skipping sweep of 4096-bit rows, degree <= 16
   if (R == 32 && d <= 16 && W == 128 * R) {
     rc = grow_device(&g.d_stamps, &g.cap_stamps, (size_t)N);
