@@ -13,11 +13,15 @@
 // a tensor-core product (dZ2, dZ1) are rounded to BF16; weight and bias
 // gradients are FP32.
 //
-// Every product is one warp per 16 x 8 output tile issuing
-// mma.sync.m16n8k16 (BF16 in, FP32 accumulate) on operands read straight
-// from L2: the largest product (4096 x 256 x 256) is about 0.5 GFLOP, far
-// below the point where staging through shared memory or the tcgen05/TMEM
-// pipeline would pay for its set-up.
+// The inference forward that ranks the proposals (4096 rows a step) is one
+// fused kernel, forward_fused_kernel: weights staged in shared memory,
+// ldmatrix-fed mma.sync.m16n8k16, both layers and the output head without a
+// round trip through memory.  The training products (at most 256 rows) are
+// one warp per 16 x 8 output tile issuing mma.sync.m16n8k16 (BF16 in, FP32
+// accumulate) on operands read straight from L2.  At these sizes (0.5 GFLOP
+// a forward pass, tiles of 32 rows) the tcgen05/TMEM pipeline's set-up --
+// TMEM allocation, descriptors, an mbarrier round trip per tile -- would not
+// pay.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -114,6 +118,197 @@ __global__ void __launch_bounds__(128) gemm_tn_kernel(int M, int N, int K, const
       e.out_b[o] = __float2bfloat16_rn(v);
       e.out_f[o] = v;
     }
+  }
+}
+
+// ---- the fused inference forward ---------------------------------------------------
+// y = w3 . relu(W2 relu(W1 x + b1) + b2) + b3 for kFuseRows rows a CTA, in one
+// launch.  The CTA stages both weight matrices (BF16) and its rows of x in
+// shared memory with one cp.async.bulk copy per row, all completing on one
+// mbarrier, each row padded by 16 bytes so that the eight 16-byte rows an
+// ldmatrix reads fall in eight different bank groups;
+// ldmatrix.x4 feeds mma.sync.m16n8k16 (BF16 in, FP32 accumulate); the first
+// hidden layer goes back to shared memory as BF16 after bias and ReLU, the
+// second is never stored: each lane applies bias, ReLU and w3 to its
+// accumulators and the row sums meet in shared memory.  Numerics as the
+// unfused path (BF16 operands, FP32 accumulation, H1 rounded to BF16); only
+// the summation order of the output dot product differs.  8 warps: warp w
+// owns rows 16 (w % 2) .. +16 and output columns 64 (w / 2) .. +64.  With
+// 64 rows and 16 warps a CTA, tensor-pipe activity rose from 16 % to 26 % of
+// active cycles, but the 4096-row pass took 12.3 us against 10.5 us: half as
+// many CTAs stage the weights.
+constexpr int kFuseRows = 32;
+constexpr int kFuseThreads = 32 * (kFuseRows / 16) * 4;   // a warp per (16-row tile, 64 columns)
+constexpr int kLdW2 = kHidden + 8;      // padded row of W2 / H1 (bf16 elements)
+constexpr int kLdW1 = kFeatures + 8;    // padded row of W1 / x
+constexpr size_t kFuseSmem = ((size_t)kHidden * kLdW2 + (size_t)kHidden * kLdW1 + (size_t)kFuseRows * kLdW1 +
+                              (size_t)kFuseRows * kLdW2) * sizeof(bf16) +
+                             (3 * (size_t)kHidden + (size_t)kFuseRows * 4) * sizeof(float);
+
+__device__ __forceinline__ void ldmatrix_x4(uint32_t (&r)[4], const bf16* p) {
+  const unsigned a = (unsigned)__cvta_generic_to_shared(p);
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+               : "r"(a));
+}
+
+// Bulk copies global -> shared (cp.async.bulk, completion on an mbarrier).
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void bulk_copy(void* dst, const void* src, unsigned bytes, unsigned bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait_parity(unsigned bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// acc[nt][4] += A (16 rows at a, row stride lda) * B^T (8 * NT rows at b, row
+// stride ldb) over K columns; A and B^T are [.][K] BF16 in shared memory.
+template <int NT, int K>
+__device__ __forceinline__ void warp_mma_tile(float (&acc)[NT][4], const bf16* a, int lda, const bf16* b, int ldb) {
+  const int lane = threadIdx.x & 31;
+  const int ar = lane & 15, ak = (lane >> 4) * 8;                 // A: rows 0-15, k halves
+  const int bn = (lane >> 4) * 8 + (lane & 7), bk = ((lane >> 3) & 1) * 8;   // B: two n-tiles, k halves
+  // unrolled: the next k-step's fragments load while this step's products issue
+#pragma unroll
+  for (int k0 = 0; k0 < K; k0 += 16) {
+    uint32_t af[4];
+    ldmatrix_x4(af, a + ar * lda + k0 + ak);
+#pragma unroll
+    for (int p = 0; p < NT / 2; ++p) {
+      uint32_t bf[4];
+      ldmatrix_x4(bf, b + (p * 16 + bn) * ldb + k0 + bk);
+      mma_16816(acc[2 * p], af[0], af[1], af[2], af[3], bf[0], bf[1]);
+      mma_16816(acc[2 * p + 1], af[0], af[1], af[2], af[3], bf[2], bf[3]);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kFuseThreads) forward_fused_kernel(const bf16* __restrict__ X, int rows,
+                                                                      const bf16* __restrict__ W1b,
+                                                                      const bf16* __restrict__ W2b,
+                                                                      const float* __restrict__ params,
+                                                                      float* __restrict__ y) {
+  extern __shared__ uint4 s_fuse[];
+  bf16* const W2s = reinterpret_cast<bf16*>(s_fuse);
+  bf16* const W1s = W2s + kHidden * kLdW2;
+  bf16* const Xs = W1s + kHidden * kLdW1;
+  bf16* const H1s = Xs + kFuseRows * kLdW1;
+  float* const b1s = reinterpret_cast<float*>(H1s + kFuseRows * kLdW2);
+  float* const b2s = b1s + kHidden;
+  float* const w3s = b2s + kHidden;
+  float* const part = w3s + kHidden;   // [kFuseRows][4] partial output sums
+  __shared__ alignas(8) unsigned long long s_bar;
+  const int r0 = blockIdx.x * kFuseRows;
+  const int valid = min(kFuseRows, rows - r0);
+  // Staging: one bulk copy per matrix row (W2: 512 bytes, W1 and x: 64 bytes)
+  // into the padded rows, all in flight at once, completing on one mbarrier.
+  const unsigned bar = smem_u32(&s_bar);
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned bytes = (unsigned)(kHidden * (kHidden + kFeatures) + valid * kFeatures) * (unsigned)sizeof(bf16);
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+  }
+  __syncthreads();
+  asm volatile("fence.proxy.async.global;" ::: "memory");
+  for (int i = threadIdx.x; i < kHidden; i += blockDim.x) {
+    bulk_copy(W2s + i * kLdW2, W2b + (long long)i * kHidden, kHidden * sizeof(bf16), bar);
+    bulk_copy(W1s + i * kLdW1, W1b + (long long)i * kFeatures, kFeatures * sizeof(bf16), bar);
+  }
+  for (int i = threadIdx.x; i < kFuseRows; i += blockDim.x) {
+    if (i < valid) {
+      bulk_copy(Xs + i * kLdW1, X + (long long)(r0 + i) * kFeatures, kFeatures * sizeof(bf16), bar);
+    } else {
+      for (int c = 0; c < kFeatures; c += 8) *reinterpret_cast<uint4*>(Xs + i * kLdW1 + c) = make_uint4(0u, 0u, 0u, 0u);
+    }
+  }
+  for (int i = threadIdx.x; i < kHidden; i += blockDim.x) {
+    b1s[i] = params[kOffB1 + i];
+    b2s[i] = params[kOffB2 + i];
+    w3s[i] = params[kOffW3 + i];
+  }
+  // bounded wait (2 s); a wait that runs out leaves NaN for this CTA's rows
+  bool staged = mbar_try_wait_parity(bar, 0u);
+  if (!staged) {
+    const unsigned long long t0 = global_ns();
+    while (!(staged = mbar_try_wait_parity(bar, 0u)))
+      if (global_ns() - t0 > 2000000000ULL) break;
+  }
+  __syncthreads();
+  if (__syncthreads_or(!staged)) {
+    if (threadIdx.x < valid) y[r0 + threadIdx.x] = __int_as_float(0x7fc00000);
+    return;
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr int kRowTiles = kFuseRows / 16;
+  const int mrow = (warp % kRowTiles) * 16, ncol = (warp / kRowTiles) * 64;
+  const int g = lane >> 2, t = lane & 3;
+  // layer 1: H1 = relu(x W1^T + b1), K = 32
+  {
+    float acc[8][4];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) acc[i][0] = acc[i][1] = acc[i][2] = acc[i][3] = 0.f;
+    warp_mma_tile<8, kFeatures>(acc, Xs + mrow * kLdW1, kLdW1, W1s + ncol * kLdW1, kLdW1);
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const int n = ncol + i * 8 + 2 * t;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int m = mrow + g + (q >= 2 ? 8 : 0), nn = n + (q & 1);
+        const float v = acc[i][q] + b1s[nn];
+        H1s[m * kLdW2 + nn] = __float2bfloat16_rn(v > 0.f ? v : 0.f);
+      }
+    }
+  }
+  __syncthreads();
+  // layer 2 and the head: y = w3 . relu(H1 W2^T + b2) + b3, K = 256
+  float acc[8][4];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) acc[i][0] = acc[i][1] = acc[i][2] = acc[i][3] = 0.f;
+  warp_mma_tile<8, kHidden>(acc, H1s + mrow * kLdW2, kLdW2, W2s + ncol * kLdW2, kLdW2);
+  float s_lo = 0.f, s_hi = 0.f;   // rows mrow + g and mrow + g + 8
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int nn = ncol + i * 8 + 2 * t + (q & 1);
+      float v = acc[i][q] + b2s[nn];
+      v = (v > 0.f ? v : 0.f) * w3s[nn];
+      if (q < 2) s_lo += v; else s_hi += v;
+    }
+  }
+#pragma unroll
+  for (int o = 1; o < 4; o <<= 1) {
+    s_lo += __shfl_xor_sync(0xffffffffu, s_lo, o);
+    s_hi += __shfl_xor_sync(0xffffffffu, s_hi, o);
+  }
+  if (t == 0) {
+    part[(mrow + g) * 4 + ncol / 64] = s_lo;
+    part[(mrow + g + 8) * 4 + ncol / 64] = s_hi;
+  }
+  __syncthreads();
+  if (threadIdx.x < valid) {
+    const float* pr = part + threadIdx.x * 4;
+    y[r0 + threadIdx.x] = ((pr[0] + pr[1]) + (pr[2] + pr[3])) + params[kOffB3];
   }
 }
 
@@ -254,6 +449,14 @@ using namespace mlp;
 
 int mlp_forward(ggb_mlp* m, const bf16* X, int rows, float* y, cudaStream_t st, bool keep_z) {
   if (rows % 16 || rows > m->max_rows) return core_fail(GGB_EINVAL, "mlp rows %d (max %d, multiple of 16)", rows, m->max_rows);
+  if (!keep_z) {
+    // inference: one fused launch, the activations never leave the SM
+    forward_fused_kernel<<<(rows + kFuseRows - 1) / kFuseRows, kFuseThreads, kFuseSmem, st>>>(X, rows, m->W1b, m->W2b,
+                                                                                            m->p, y);
+    core_add_launches(1);
+    MCUDA(cudaGetLastError());
+    return GGB_OK;
+  }
   EpiArgs e1 = {m->p + kOffB1, nullptr, m->H1, nullptr, nullptr};
   gemm_tn_kernel<kEpiBiasReluBf16><<<blocks_for((long long)(rows / 16) * (kHidden / 8)), 128, 0, st>>>(
       rows, kHidden, kFeatures, X, kFeatures, m->W1b, kFeatures, e1);
@@ -348,6 +551,8 @@ int create(ggb_mlp* m, int max_rows, unsigned long long seed) {
   using namespace ggb::mlp;
   m->max_rows = max_rows;
   int rc;
+  MCUDA(cudaFuncSetAttribute((const void*)forward_fused_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)kFuseSmem));
   const size_t R = (size_t)max_rows;
   if ((rc = mdev(&m->p, kParams)) || (rc = mdev(&m->g, kParams)) || (rc = mdev(&m->m1, kParams)) ||
       (rc = mdev(&m->m2, kParams)) || (rc = mdev(&m->step, 1)) || (rc = mdev(&m->W1b, (size_t)kOffB1)) ||
