@@ -22,6 +22,8 @@
 #include <cstdint>
 #include <mutex>
 
+#include <immintrin.h>
+
 #include "../../include/graphgolf_b200.h"
 #include "apsp_kernel.cuh"
 #include "core_internal.h"
@@ -463,6 +465,25 @@ int check_general(int nodes, int based_nodes, int groups, int degree, int added_
   return GGB_OK;
 }
 
+// Copies n ints with 32-byte non-temporal stores (dst 32-byte aligned): the
+// pinned staging buffer is never read by the CPU, so its lines need not be
+// read for ownership or kept in the caches.
+__attribute__((target("avx2"))) void copy_stream(int* dst, const int* src, size_t n) {
+  size_t i = 0;
+  for (; i + 32 <= n; i += 32) {
+    const __m256i a = _mm256_loadu_si256(reinterpret_cast<const __m256i*>(src + i));
+    const __m256i b = _mm256_loadu_si256(reinterpret_cast<const __m256i*>(src + i + 8));
+    const __m256i c = _mm256_loadu_si256(reinterpret_cast<const __m256i*>(src + i + 16));
+    const __m256i d = _mm256_loadu_si256(reinterpret_cast<const __m256i*>(src + i + 24));
+    _mm256_stream_si256(reinterpret_cast<__m256i*>(dst + i), a);
+    _mm256_stream_si256(reinterpret_cast<__m256i*>(dst + i + 8), b);
+    _mm256_stream_si256(reinterpret_cast<__m256i*>(dst + i + 16), c);
+    _mm256_stream_si256(reinterpret_cast<__m256i*>(dst + i + 24), d);
+  }
+  for (; i < n; ++i) dst[i] = src[i];
+  _mm_sfence();
+}
+
 int stage_adj(const int* adj, size_t n, cudaStream_t st) {
   int rc = grow_device(&g.d_adj, &g.cap_adj, n);
   if (rc) return rc;
@@ -471,12 +492,19 @@ int stage_adj(const int* adj, size_t n, cudaStream_t st) {
   if (n) {
     // The pinned copy must not be overwritten while a previous copy from it is
     // in flight: the stream is idle here (every host entry point waits).
-    // Chunks of at most 512 KiB: the copy of chunk i into the pinned buffer
-    // overlaps the DMA of chunk i-1.
+    // Chunks of 512 KiB: the copy of chunk i into the pinned buffer overlaps
+    // the DMA of chunk i-1.  The copy uses non-temporal stores where the CPU
+    // has AVX2 (measured on the GPU box's host: 482-484 evals/s end to end at
+    // N=65536, d=16, against 456 with memcpy; sending 16-bit ids instead was
+    // within the noise of it).
+    static const bool avx2 = __builtin_cpu_supports("avx2");
     const size_t chunk = (size_t)128 * 1024;   // ints
     for (size_t o = 0; o < n; o += chunk) {
       const size_t m = std::min(chunk, n - o);
-      std::memcpy(g.h_adj + o, adj + o, m * sizeof(int));
+      if (avx2)
+        copy_stream(g.h_adj + o, adj + o, m);
+      else
+        std::memcpy(g.h_adj + o, adj + o, m * sizeof(int));
       CUDA_TRY(cudaMemcpyAsync(g.d_adj + o, g.h_adj + o, m * sizeof(int), cudaMemcpyHostToDevice, st));
     }
   }
