@@ -401,7 +401,9 @@ int create(int n_graphs, const int* nodes, const int* based_nodes, const int* gr
     gs[i].n_src = b->bn[i];
     gs[i].groups = b->grp[i];
     gs[i].vec4 = (b->d[i] % 4 == 0) ? 1 : 0;   // every graph starts on a 16-byte boundary
-    gs[i].pad_ = 0;
+    gs[i].win_first = 0;
+    gs[i].win_stride = 1;
+    gs[i].win_bits = 0;
   }
   BCUDA(cudaMemcpy(b->d_graphs, gs.data(), gs.size() * sizeof(ggb::BatchGraph), cudaMemcpyHostToDevice));
   BCUDA(cudaMemset(b->d_adj, 0, std::max<size_t>((size_t)b->adj_ints, 1) * sizeof(int)));

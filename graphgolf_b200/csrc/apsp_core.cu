@@ -130,7 +130,17 @@ struct State {
   int trace_cap = 0;
   int trace_len = 0;
   int occ[8] = {0, 0, 0, 0, 0, 0, 0, 0};   // co-resident CTAs per SM, per R index
+  int tocc[4] = {0, 0, 0, 0};             // the same for the window-team kernel, R = 1, 2, 4, 8
   int smem_optin = 0;
+  // window teams (narrow windows of one graph, several at a time): the batch
+  // kernel's per-team entries, results and control blocks, and pinned staging
+  ggb::BatchGraph* d_tgraphs = nullptr;
+  ggb::BatchOut* d_tout = nullptr;
+  ggb::ApspCtrl* d_tctrl = nullptr;
+  int* d_tint = nullptr;          // team_start [kMaxTeams + 1], team_list [kMaxTeams]
+  long long* d_tll = nullptr;     // team_off [kMaxTeams], team_cells [kMaxTeams]
+  unsigned char* h_team = nullptr;   // pinned: the above for upload, then results for read-back
+  int last_teams = 0;
   // last launch bookkeeping (for ggb_collect)
   int last_N = 0, last_R = 0, last_W = 0;
   bool pending = false;
@@ -191,6 +201,18 @@ size_t smem_for(int R) {
   }
 }
 
+constexpr int kMaxTeams = 256;
+
+const void* team_kernel_for(int R) {
+  switch (R) {
+    case 1: return (const void*)ggb::apsp_batch_kernel<1>;
+    case 2: return (const void*)ggb::apsp_batch_kernel<2>;
+    case 4: return (const void*)ggb::apsp_batch_kernel<4>;
+    case 8: return (const void*)ggb::apsp_batch_kernel<8>;
+    default: return nullptr;
+  }
+}
+
 int ensure_ready(int device) {
   if (g.ready) return GGB_OK;
   if (device < 0) {
@@ -216,6 +238,11 @@ int ensure_ready(int device) {
     CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel_for(R), ggb::kThreads, smem_for(R)));
     if (nb < 1) return fail(GGB_ECUDA, "persistent kernel R=%d cannot be resident", R);
     g.occ[r_index(R)] = nb;
+  }
+  for (int R = 1; R <= 8; R *= 2) {
+    int nb = 0;
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, team_kernel_for(R), ggb::kThreads, smem_for(R)));
+    g.tocc[r_index(R)] = nb;
   }
   int smem_optin = 0;
   CUDA_TRY(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
@@ -288,11 +315,111 @@ int choose_R(int N, int d, int nsrc_max) {
   return bestR;
 }
 
+size_t team_pinned_bytes() {
+  return kMaxTeams * (sizeof(ggb::BatchGraph) + sizeof(ggb::BatchOut) + sizeof(ggb::ApspCtrl)) +
+         (2 * kMaxTeams + 2) * sizeof(int) + 2 * kMaxTeams * sizeof(long long) + 256;
+}
+
+// Narrow windows of one graph on teams of CTAs: team j of T runs this rank's
+// windows rank + procs*j, rank + procs*(j + T), ... with its own grid barrier
+// and its own two window matrices, so the per-window latency (seeding, a
+// barrier per level) of T windows overlaps.  The batch kernel does the work;
+// its answer per team is a partial like a rank's.
+int launch_teams(const int* d_adj, int N, int d, int n_src1, int groups, int rank, int procs, int R, int W, int T,
+                 int team_ctas, bool vec4, cudaStream_t st) {
+  const size_t cells = (size_t)N * R;
+  int rc = grow_device(&g.d_bufs, &g.cap_buf, 2 * cells * T);
+  if (rc) return rc;
+  if (!g.d_tgraphs) {
+    CUDA_TRY(cudaMalloc(&g.d_tgraphs, kMaxTeams * sizeof(ggb::BatchGraph)));
+    CUDA_TRY(cudaMalloc(&g.d_tout, kMaxTeams * sizeof(ggb::BatchOut)));
+    CUDA_TRY(cudaMalloc(&g.d_tctrl, kMaxTeams * sizeof(ggb::ApspCtrl)));
+    CUDA_TRY(cudaMalloc(&g.d_tint, (2 * kMaxTeams + 1) * sizeof(int)));
+    CUDA_TRY(cudaMalloc(&g.d_tll, 2 * kMaxTeams * sizeof(long long)));
+    CUDA_TRY(cudaHostAlloc(&g.h_team, team_pinned_bytes(), cudaHostAllocDefault));
+  }
+  // the previous launch's read-back is complete: every host entry point waits
+  ggb::BatchGraph* hg = reinterpret_cast<ggb::BatchGraph*>(g.h_team);
+  int* hi = reinterpret_cast<int*>(hg + kMaxTeams);
+  long long* hl = reinterpret_cast<long long*>(hi + 2 * kMaxTeams + 2);
+  for (int j = 0; j < T; ++j) {
+    hg[j].adj = d_adj;
+    hg[j].N = N;
+    hg[j].d = d;
+    hg[j].n_src = n_src1;
+    hg[j].groups = groups;
+    hg[j].vec4 = vec4 ? 1 : 0;
+    hg[j].win_first = rank + procs * j;
+    hg[j].win_stride = procs * T;
+    hg[j].win_bits = W < 128 * R ? W : 0;
+    hi[j] = j;                      // team_start
+    hi[kMaxTeams + 1 + j] = j;      // team_list
+    hl[j] = (long long)(2 * cells) * j;   // team_off
+    hl[kMaxTeams + j] = (long long)cells; // team_cells
+  }
+  hi[T] = T;
+  CUDA_TRY(cudaMemcpyAsync(g.d_tgraphs, hg, T * sizeof(ggb::BatchGraph), cudaMemcpyHostToDevice, st));
+  CUDA_TRY(cudaMemcpyAsync(g.d_tint, hi, (2 * kMaxTeams + 1) * sizeof(int), cudaMemcpyHostToDevice, st));
+  CUDA_TRY(cudaMemcpyAsync(g.d_tll, hl, 2 * kMaxTeams * sizeof(long long), cudaMemcpyHostToDevice, st));
+  CUDA_TRY(cudaMemsetAsync(g.d_tctrl, 0, T * sizeof(ggb::ApspCtrl), st));
+  CUDA_TRY(cudaMemsetAsync(g.d_tout, 0, T * sizeof(ggb::BatchOut), st));
+  ggb::BatchArgs b;
+  b.graphs = g.d_tgraphs;
+  b.out = g.d_tout;
+  b.team_ctrl = g.d_tctrl;
+  b.team_start = g.d_tint;
+  b.team_list = g.d_tint + kMaxTeams + 1;
+  b.scratch = g.d_bufs;
+  b.team_off = g.d_tll;
+  b.team_cells = g.d_tll + kMaxTeams;
+  b.timeout_ns = g.timeout_ns;
+  b.stop = nullptr;
+  b.sticky = nullptr;
+  b.n_teams = T;
+  b.team_ctas = team_ctas;
+  if (g.timing) {
+    CUDA_TRY(cudaEventRecord(g.ev[0], st));
+    CUDA_TRY(cudaEventRecord(g.ev[1], st));
+  }
+  void* params[] = {(void*)&b};
+  CUDA_TRY(cudaLaunchCooperativeKernel(team_kernel_for(R), dim3(T * team_ctas), dim3(ggb::kThreads), params,
+                                       smem_for(R), st));
+  ++g_launches;
+  if (g.timing) CUDA_TRY(cudaEventRecord(g.ev[2], st));
+  g.ev_ball = false;
+  g.last_N = N;
+  g.last_R = R;
+  g.last_W = W;
+  g.last_teams = T;
+  g.pending = true;
+  return GGB_OK;
+}
+
 int launch_apsp(const int* d_adj, int N, int d, int n_src1, int split, int ac, int groups,
                 int rank, int procs, cudaStream_t st, const int* d_adj2 = nullptr) {
   const int R = choose_R(N, d, std::max(n_src1, ac));
   const int ri = r_index(R);
   if (ri < 0) return fail(GGB_EINVAL, "window of %d uint4 per row is not supported", R);
+  g.last_teams = 0;
+  {
+    // narrow windows (rows of at most 128 bytes), no added centres: teams of
+    // windows when at least two fit in the L2 budget and there are windows
+    // enough for them
+    const int Wt = (R == 1 && g.force_W > 0) ? g.force_W : 128 * R;
+    const int nwin1t = n_src1 > 0 ? (n_src1 + Wt - 1) / Wt : 0;
+    const int n_loc = nwin1t > rank ? (nwin1t - rank + procs - 1) / procs : 0;
+    const double budget = std::max<double>(8.0 * 1024 * 1024, (double)g.l2_bytes * 0.55);
+    const long long fit = (long long)(budget / (2.0 * N * 16.0 * R));
+    const int total = R <= 8 ? std::min(max_ctas(R), g.tocc[r_index(R)] * g.sms) : 0;
+    int T = (int)std::min<long long>(std::min<long long>(fit, n_loc), std::min(total / 2, kMaxTeams));
+    if (R <= 8 && ac == 0 && !d_adj2 && g.force_ctas == 0 && T >= 2 && n_loc >= 4) {
+      const int team_ctas = total / T;
+      T = total / team_ctas;   // every CTA in a team
+      T = std::min<long long>(std::min<long long>(T, fit), std::min(n_loc, kMaxTeams));
+      const bool vec4t = (d % 4 == 0 && ((uintptr_t)d_adj % 16) == 0);
+      return launch_teams(d_adj, N, d, n_src1, groups, rank, procs, R, Wt, T, team_ctas, vec4t, st);
+    }
+  }
   const size_t cells = (size_t)N * R;
   // Both matrices live in one allocation: buf0 = [0, cells), buf1 = [cells, 2*cells).
   int rc = grow_device(&g.d_bufs, &g.cap_buf, 2 * cells);
@@ -408,7 +535,47 @@ int launch_apsp(const int* d_adj, int N, int d, int n_src1, int split, int ac, i
   return GGB_OK;
 }
 
+// The teams' results joined into one partial (MAX diameter, SUM of the
+// sums), after their errors.
+int read_teams(cudaStream_t st, ggb_partial* p) {
+  const int T = g.last_teams;
+  ggb::BatchGraph* hg = reinterpret_cast<ggb::BatchGraph*>(g.h_team);
+  long long* hl = reinterpret_cast<long long*>(reinterpret_cast<int*>(hg + kMaxTeams) + 2 * kMaxTeams + 2);
+  ggb::BatchOut* ho = reinterpret_cast<ggb::BatchOut*>(hl + 2 * kMaxTeams);
+  ApspCtrl* hc = reinterpret_cast<ApspCtrl*>(ho + kMaxTeams);
+  CUDA_TRY(cudaMemcpyAsync(ho, g.d_tout, T * sizeof(ggb::BatchOut), cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaMemcpyAsync(hc, g.d_tctrl, T * sizeof(ApspCtrl), cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  g.pending = false;
+  g.trace_len = 0;
+  for (int j = 0; j < T; ++j) {
+    const ApspCtrl& c = hc[j];
+    if (c.error == ggb::kErrAdj)
+      return fail(GGB_EADJ, "adjacency entry outside [0, nodes) (reported by CTA/vertex %d)", c.error_info);
+    if (c.error == ggb::kErrTimeout) return fail(GGB_ETIMEOUT, "a team barrier wait ran out (CTA %d)", c.error_info);
+    if (c.error != 0) return fail(GGB_ECUDA, "device error code %d", c.error);
+    if (!ho[j].done) return fail(GGB_ECUDA, "window team %d did not complete", j);
+  }
+  p->diam = 1;
+  p->disconnected = 0;
+  p->sum = 0;
+  p->levels = 0;
+  p->dense_levels = 0;
+  p->windows = 0;
+  for (int j = 0; j < T; ++j) {
+    p->diam = std::max(p->diam, ho[j].diam);
+    p->disconnected |= ho[j].disconnected;
+    p->sum += ho[j].sum;
+    p->levels += ho[j].levels;
+    p->dense_levels += ho[j].dense_levels;
+    p->windows += ho[j].windows;
+  }
+  p->window_bits = g.last_W;
+  return GGB_OK;
+}
+
 int read_ctrl(cudaStream_t st, ggb_partial* p) {
+  if (g.last_teams > 0) return read_teams(st, p);
   CUDA_TRY(cudaMemcpyAsync(g.h_ctrl, g.d_ctrl, sizeof(ApspCtrl), cudaMemcpyDeviceToHost, st));
   CUDA_TRY(cudaStreamSynchronize(st));
   g.pending = false;
@@ -569,6 +736,12 @@ void ggb_finalize(void) {
     if (e) cudaEventDestroy(e);
   cudaFree(g.d_ball);
   cudaFree(g.d_ball_cnt);
+  cudaFree(g.d_tgraphs);
+  cudaFree(g.d_tout);
+  cudaFree(g.d_tctrl);
+  cudaFree(g.d_tint);
+  cudaFree(g.d_tll);
+  cudaFreeHost(g.h_team);
   cudaFree(g.d_stamps);
   cudaFreeHost(g.h_adj);
   cudaFreeHost(g.h_rh);

@@ -1331,7 +1331,9 @@ struct BatchGraph {
   int n_src;             // phase-1 sources (based_nodes); N = n_src * groups
   int groups;
   int vec4;              // d % 4 == 0 and adj 16-byte aligned
-  int pad_;
+  int win_first;         // the graph's source windows this entry runs: win_first, win_first + win_stride,
+  int win_stride;        // ... (0, 1: all of them; one graph's windows spread over teams otherwise)
+  int win_bits;          // sources per window below 128 * R (64), or 0
 };
 
 struct BatchOut {        // per graph, written by the team's first CTA
@@ -1371,8 +1373,6 @@ __global__ void __launch_bounds__(kThreads, 1) apsp_batch_kernel(const BatchArgs
   a.ctrl = b.team_ctrl + team;
   a.timeout_ns = b.timeout_ns;
   a.ac = 0;
-  a.win_first = 0;
-  a.win_stride = 1;
   a.ball = nullptr;
   a.ball_cnt = nullptr;
   a.trace = nullptr;
@@ -1397,6 +1397,9 @@ __global__ void __launch_bounds__(kThreads, 1) apsp_batch_kernel(const BatchArgs
     a.split = gr.N;
     a.groups = gr.groups;
     a.vec4 = gr.vec4;
+    a.win_first = gr.win_first;
+    a.win_stride = gr.win_stride;
+    a.win_bits = gr.win_bits;
     EvalOut o;
     if (!eval_windows<R>(a, cta, b.team_ctas, sm, s_dyn, bar_target, gl, ntrace, o)) {
       if (b.sticky && threadIdx.x == 0) atomicCAS(b.sticky, 0, max(1, ld_volatile_i32(&a.ctrl->error)));
