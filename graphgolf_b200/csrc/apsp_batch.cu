@@ -489,7 +489,7 @@ int ggb_batch_upload(ggb_batch* b, const int* const* adj, void* stream) {
   long long pending = 0;                 // first int not yet sent
   for (int i = 0; i < b->n; ++i) {
     const size_t n = (size_t)b->N[i] * b->d[i];
-    if (n) std::memcpy(b->h_adj + b->off[i], adj[i], n * sizeof(int));
+    if (n) ggb::stage_copy(b->h_adj + b->off[i], adj[i], n);
     const long long end = i + 1 < b->n ? b->off[i + 1] : b->adj_ints;
     if (end - pending >= flush || i + 1 == b->n) {
       BCUDA(cudaMemcpyAsync(b->d_adj + pending, b->h_adj + pending, (size_t)(end - pending) * sizeof(int),

@@ -632,11 +632,12 @@ int check_general(int nodes, int based_nodes, int groups, int degree, int added_
   return GGB_OK;
 }
 
-// Copies n ints with 32-byte non-temporal stores (dst 32-byte aligned): the
-// pinned staging buffer is never read by the CPU, so its lines need not be
-// read for ownership or kept in the caches.
+// Copies n ints with 32-byte non-temporal stores: the pinned staging buffer
+// is never read by the CPU, so its lines need not be read for ownership or
+// kept in the caches.  dst needs 4-byte alignment only.
 __attribute__((target("avx2"))) void copy_stream(int* dst, const int* src, size_t n) {
   size_t i = 0;
+  for (; i < n && ((uintptr_t)(dst + i) & 31u); ++i) dst[i] = src[i];
   for (; i + 32 <= n; i += 32) {
     const __m256i a = _mm256_loadu_si256(reinterpret_cast<const __m256i*>(src + i));
     const __m256i b = _mm256_loadu_si256(reinterpret_cast<const __m256i*>(src + i + 8));
@@ -651,6 +652,22 @@ __attribute__((target("avx2"))) void copy_stream(int* dst, const int* src, size_
   _mm_sfence();
 }
 
+}  // namespace
+
+namespace ggb {
+
+void stage_copy(int* dst, const int* src, size_t n) {
+  static const bool avx2 = __builtin_cpu_supports("avx2");
+  if (avx2)
+    copy_stream(dst, src, n);
+  else
+    std::memcpy(dst, src, n * sizeof(int));
+}
+
+}  // namespace ggb
+
+namespace {
+
 int stage_adj(const int* adj, size_t n, cudaStream_t st) {
   int rc = grow_device(&g.d_adj, &g.cap_adj, n);
   if (rc) return rc;
@@ -664,14 +681,10 @@ int stage_adj(const int* adj, size_t n, cudaStream_t st) {
     // has AVX2 (measured on the GPU box's host: 482-484 evals/s end to end at
     // N=65536, d=16, against 456 with memcpy; sending 16-bit ids instead was
     // within the noise of it).
-    static const bool avx2 = __builtin_cpu_supports("avx2");
     const size_t chunk = (size_t)128 * 1024;   // ints
     for (size_t o = 0; o < n; o += chunk) {
       const size_t m = std::min(chunk, n - o);
-      if (avx2)
-        copy_stream(g.h_adj + o, adj + o, m);
-      else
-        std::memcpy(g.h_adj + o, adj + o, m * sizeof(int));
+      ggb::stage_copy(g.h_adj + o, adj + o, m);
       CUDA_TRY(cudaMemcpyAsync(g.d_adj + o, g.h_adj + o, m * sizeof(int), cudaMemcpyHostToDevice, st));
     }
   }
