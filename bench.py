@@ -615,6 +615,7 @@ def run_sharded(args, wl, lib, rank: int, world: int, local: int, dist) -> int:
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
+    launches0 = lib.ggb_kernel_launches()
     with Clocks(local) as clk:
         for k in range(args.steps):
             r = step(evs[k])
@@ -636,7 +637,7 @@ def run_sharded(args, wl, lib, rank: int, world: int, local: int, dist) -> int:
                        "parallelism": f"source windows of one graph over {world} ranks, 16-byte all-reduce"},
             "run": {"diameter": first.diameter, "total": first.total, "windows_per_rank": part.windows,
                     "window_bits": part.window_bits},
-            "gpu_launches": None, "clocks": clk.summary()}
+            "gpu_launches": int(lib.ggb_kernel_launches() - launches0), "clocks": clk.summary()}
     if rank == 0:
         print(json.dumps(line))
     if dist:
