@@ -64,3 +64,25 @@ def test_pure_python_generator_reproduces_the_headline_graphs():
         else:
             e = graphgen.symmetric_regular_edges(p["n"], p["d"], c["groups"], c["seed"])
         assert adj_hash(graphgen.create_adj(p["n"], p["d"], e)) == c["adj_sha"]
+
+
+def test_grid_trajectory_fixture_matches_the_generator(tmp_path):
+    """The committed 100 000-step grid trajectory was recorded on the input
+    the seeded lattice generator gives today, and holds one progress row per
+    1 000 steps plus the final result lines."""
+    import hashlib
+    import json
+    import sys
+    from pathlib import Path
+    gold = Path(__file__).resolve().parent / "golden"
+    want = json.loads((gold / "grid_trajectory_w100h100d4r3.json").read_text())
+    sys.path.insert(0, str(gold))
+    from make_grid_trajectory import CONFIG, write_input
+    assert want["config"] == CONFIG
+    f = tmp_path / "in.edges"
+    write_input(str(f))
+    assert hashlib.sha256(f.read_bytes()).hexdigest() == want["input_sha256"]
+    rows = [l for l in want["lines"] if l.split() and l.split()[0].isdigit()]
+    assert [int(r.split()[0]) for r in rows] == list(range(0, CONFIG["steps"], 1000))
+    assert any(l.startswith("Diam. k") for l in want["lines"])
+    assert any(l.startswith("Accept rate") for l in want["lines"])
