@@ -37,7 +37,7 @@ OUT = Path(__file__).resolve().parent / "grid_trajectory_w100h100d4r3.json"
 CONFIG = {"width": 100, "height": 100, "degree": 4, "length": 3, "graph_seed": 1, "sa_seed": 1, "steps": 100000}
 
 _DROP = ("Run on", "sec", "---", "Seed", "Num. of threads", "Threads", "Processes", "Num. of processes",
-         "Output filename")
+         "Output filename", "Input filename")
 
 
 def stable_lines(text: str) -> list[str]:
