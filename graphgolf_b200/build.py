@@ -55,7 +55,8 @@ def _run(cmd: list[str]) -> None:
 
 
 def core_sources() -> list[Path]:
-    return sorted(CSRC.glob("*.cu")) + sorted(CSRC.glob("*.cuh")) + [INCLUDE / "graphgolf_b200.h"]
+    return [*sorted(CSRC.glob("*.cu")), *sorted(CSRC.glob("*.cuh")), *sorted(CSRC.glob("*.h")),
+            INCLUDE / "graphgolf_b200.h"]
 
 
 def build(verbose: bool = False) -> dict[str, Path]:

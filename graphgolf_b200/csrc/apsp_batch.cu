@@ -483,20 +483,11 @@ int ggb_batch_upload(ggb_batch* b, const int* const* adj, void* stream) {
   BCUDA(cudaStreamSynchronize(st));
   for (int i = 0; i < b->n; ++i)
     if ((size_t)b->N[i] * b->d[i] && !adj[i]) return core_fail(GGB_EINVAL, "batch graph %d: null adjacency", i);
-  // Each graph's copy into the pinned buffer overlaps the DMA of the graphs
-  // before it (one DMA per ~512 KiB of staged graphs).
-  const long long flush = 128 * 1024;   // ints
-  long long pending = 0;                 // first int not yet sent
-  for (int i = 0; i < b->n; ++i) {
-    const size_t n = (size_t)b->N[i] * b->d[i];
-    if (n) ggb::stage_copy(b->h_adj + b->off[i], adj[i], n);
-    const long long end = i + 1 < b->n ? b->off[i + 1] : b->adj_ints;
-    if (end - pending >= flush || i + 1 == b->n) {
-      BCUDA(cudaMemcpyAsync(b->d_adj + pending, b->h_adj + pending, (size_t)(end - pending) * sizeof(int),
-                            cudaMemcpyHostToDevice, st));
-      pending = end;
-    }
-  }
+  // The copy into the pinned buffer is spread over the staging threads; each
+  // unit of about 512 KiB or more is sent as soon as it is copied (stage.cu).
+  std::vector<ggb::StageSeg> segs(b->n);
+  for (int i = 0; i < b->n; ++i) segs[i] = {adj[i], (size_t)b->off[i], (size_t)b->N[i] * b->d[i]};
+  BCUDA(ggb::stage_upload(b->device, b->h_adj, b->d_adj, segs.data(), b->n, (size_t)b->adj_ints, st));
   return GGB_OK;
 }
 

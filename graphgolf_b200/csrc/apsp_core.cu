@@ -22,8 +22,6 @@
 #include <cstdint>
 #include <mutex>
 
-#include <immintrin.h>
-
 #include "../../include/graphgolf_b200.h"
 #include "apsp_kernel.cuh"
 #include "core_internal.h"
@@ -632,62 +630,17 @@ int check_general(int nodes, int based_nodes, int groups, int degree, int added_
   return GGB_OK;
 }
 
-// Copies n ints with 32-byte non-temporal stores: the pinned staging buffer
-// is never read by the CPU, so its lines need not be read for ownership or
-// kept in the caches.  dst needs 4-byte alignment only.
-__attribute__((target("avx2"))) void copy_stream(int* dst, const int* src, size_t n) {
-  size_t i = 0;
-  for (; i < n && ((uintptr_t)(dst + i) & 31u); ++i) dst[i] = src[i];
-  for (; i + 32 <= n; i += 32) {
-    const __m256i a = _mm256_loadu_si256(reinterpret_cast<const __m256i*>(src + i));
-    const __m256i b = _mm256_loadu_si256(reinterpret_cast<const __m256i*>(src + i + 8));
-    const __m256i c = _mm256_loadu_si256(reinterpret_cast<const __m256i*>(src + i + 16));
-    const __m256i d = _mm256_loadu_si256(reinterpret_cast<const __m256i*>(src + i + 24));
-    _mm256_stream_si256(reinterpret_cast<__m256i*>(dst + i), a);
-    _mm256_stream_si256(reinterpret_cast<__m256i*>(dst + i + 8), b);
-    _mm256_stream_si256(reinterpret_cast<__m256i*>(dst + i + 16), c);
-    _mm256_stream_si256(reinterpret_cast<__m256i*>(dst + i + 24), d);
-  }
-  for (; i < n; ++i) dst[i] = src[i];
-  _mm_sfence();
-}
-
-}  // namespace
-
-namespace ggb {
-
-void stage_copy(int* dst, const int* src, size_t n) {
-  static const bool avx2 = __builtin_cpu_supports("avx2");
-  if (avx2)
-    copy_stream(dst, src, n);
-  else
-    std::memcpy(dst, src, n * sizeof(int));
-}
-
-}  // namespace ggb
-
-namespace {
-
 int stage_adj(const int* adj, size_t n, cudaStream_t st) {
   int rc = grow_device(&g.d_adj, &g.cap_adj, n);
   if (rc) return rc;
   rc = grow_pinned(&g.h_adj, &g.cap_hadj, n);
   if (rc) return rc;
-  if (n) {
-    // The pinned copy must not be overwritten while a previous copy from it is
-    // in flight: the stream is idle here (every host entry point waits).
-    // Chunks of 512 KiB: the copy of chunk i into the pinned buffer overlaps
-    // the DMA of chunk i-1.  The copy uses non-temporal stores where the CPU
-    // has AVX2 (measured on the GPU box's host: 482-484 evals/s end to end at
-    // N=65536, d=16, against 456 with memcpy; sending 16-bit ids instead was
-    // within the noise of it).
-    const size_t chunk = (size_t)128 * 1024;   // ints
-    for (size_t o = 0; o < n; o += chunk) {
-      const size_t m = std::min(chunk, n - o);
-      ggb::stage_copy(g.h_adj + o, adj + o, m);
-      CUDA_TRY(cudaMemcpyAsync(g.d_adj + o, g.h_adj + o, m * sizeof(int), cudaMemcpyHostToDevice, st));
-    }
-  }
+  // The pinned copy must not be overwritten while a previous copy from it is
+  // in flight: the stream is idle here (every host entry point waits).  The
+  // copy into pinned memory is spread over the staging threads, each unit's
+  // DMA enqueued as soon as it is copied (stage.cu).
+  const ggb::StageSeg seg = {adj, 0, n};
+  CUDA_TRY(ggb::stage_upload(g.device, g.h_adj, g.d_adj, &seg, 1, n, st));
   return GGB_OK;
 }
 

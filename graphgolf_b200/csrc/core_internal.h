@@ -3,6 +3,8 @@
 // ggb_kernel_launches() reports, and the host copy into pinned staging.
 // Not part of the public C ABI.
 #pragma once
+#include <cuda_runtime.h>
+
 #include <cstddef>
 
 namespace ggb {
@@ -16,5 +18,24 @@ void core_add_launches(long long n);
 // Copies n ints from pageable memory into pinned staging (non-temporal
 // stores where the CPU has AVX2, memcpy otherwise).
 void stage_copy(int* dst, const int* src, size_t n);
+
+// One source array of an upload: it fills ints [off, off + n) of the pinned
+// and device buffers.
+struct StageSeg {
+  const int* src;
+  size_t off;
+  size_t n;
+};
+
+// Copies the segments into the pinned buffer and enqueues the host-to-device
+// copy of ints [0, total) of it into `dev` on stream st of `device`, spread
+// over the staging threads (stage.cu).  total must cover every segment; ints
+// between segments are sent as they lie in the pinned buffer.  The pinned
+// buffer must not feed a copy still in flight.  Returns the first CUDA error.
+cudaError_t stage_upload(int device, int* pinned, int* dev, const StageSeg* segs, int nsegs, size_t total,
+                         cudaStream_t st);
+
+// Number of threads stage_upload() copies with, the caller included.
+int stage_threads();
 
 }  // namespace ggb
