@@ -316,6 +316,7 @@ void destroy(ggb_batch* b) {
   if (b->stream) cudaStreamSynchronize(b->stream);
   drop_graph(b);
   cudaFree(b->d_adj);
+  cudaFree(b->d_adj16);
   cudaFreeHost(b->h_adj);
   cudaFree(b->d_graphs);
   cudaFree(b->d_out);
@@ -383,6 +384,10 @@ int create(int n_graphs, const int* nodes, const int* based_nodes, const int* gr
     b->h_adj = nullptr;
     return core_fail(GGB_ENOMEM, "pinned staging of %lld ints failed", b->adj_ints);
   }
+  // Graphs of at most 65536 vertices have 16-bit ids: uploads send them narrowed.
+  if (*std::max_element(b->N.begin(), b->N.end()) <= 65536 &&
+      (rc = dev_alloc(&b->d_adj16, (size_t)b->adj_ints)))
+    return rc;
   if ((rc = dev_alloc(&b->d_graphs, (size_t)n_graphs))) return rc;
   if ((rc = dev_alloc(&b->d_out, (size_t)n_graphs))) return rc;
   const size_t mt = (size_t)b->max_teams;
@@ -484,10 +489,12 @@ int ggb_batch_upload(ggb_batch* b, const int* const* adj, void* stream) {
   for (int i = 0; i < b->n; ++i)
     if ((size_t)b->N[i] * b->d[i] && !adj[i]) return core_fail(GGB_EINVAL, "batch graph %d: null adjacency", i);
   // The copy into the pinned buffer is spread over the staging threads; each
-  // unit of about 512 KiB or more is sent as soon as it is copied (stage.cu).
+  // unit of 128 Ki ids or more is sent as soon as it is copied, as 16-bit ids
+  // when they fit (stage.cu).
   std::vector<ggb::StageSeg> segs(b->n);
   for (int i = 0; i < b->n; ++i) segs[i] = {adj[i], (size_t)b->off[i], (size_t)b->N[i] * b->d[i]};
-  BCUDA(ggb::stage_upload(b->device, b->h_adj, b->d_adj, segs.data(), b->n, (size_t)b->adj_ints, st));
+  BCUDA(ggb::stage_upload_ids(b->device, b->h_adj, b->d_adj16, b->d_adj, segs.data(), b->n, (size_t)b->adj_ints,
+                              st));
   return GGB_OK;
 }
 

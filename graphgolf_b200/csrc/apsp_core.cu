@@ -98,6 +98,7 @@ struct State {
   cudaStream_t stream = nullptr;
   // device buffers (grow-only)
   int* d_adj = nullptr;       size_t cap_adj = 0;     // ints
+  uint16_t* d_adj16 = nullptr; size_t cap_adj16 = 0; // 16-bit ids on their way to d_adj
   int* d_adj2 = nullptr;      size_t cap_adj2 = 0;    // ints (grid relabel)
   int* d_rh = nullptr;        size_t cap_rh = 0;      // ints
   int* d_inv = nullptr;       size_t cap_inv = 0;     // ints
@@ -630,17 +631,22 @@ int check_general(int nodes, int based_nodes, int groups, int degree, int added_
   return GGB_OK;
 }
 
-int stage_adj(const int* adj, size_t n, cudaStream_t st) {
+int stage_adj(const int* adj, size_t n, int nodes, cudaStream_t st) {
   int rc = grow_device(&g.d_adj, &g.cap_adj, n);
   if (rc) return rc;
   rc = grow_pinned(&g.h_adj, &g.cap_hadj, n);
   if (rc) return rc;
+  // Valid ids of a graph with at most 65536 vertices fit 16 bits: send them
+  // narrowed (half the PCIe bytes) and widen them on the device (stage.cu).
+  uint16_t* d16 = nullptr;
+  if (nodes <= 65536) {
+    if ((rc = grow_device(&g.d_adj16, &g.cap_adj16, n))) return rc;
+    d16 = g.d_adj16;
+  }
   // The pinned copy must not be overwritten while a previous copy from it is
-  // in flight: the stream is idle here (every host entry point waits).  The
-  // copy into pinned memory is spread over the staging threads, each unit's
-  // DMA enqueued as soon as it is copied (stage.cu).
+  // in flight: the stream is idle here (every host entry point waits).
   const ggb::StageSeg seg = {adj, 0, n};
-  CUDA_TRY(ggb::stage_upload(g.device, g.h_adj, g.d_adj, &seg, 1, n, st));
+  CUDA_TRY(ggb::stage_upload_ids(g.device, g.h_adj, d16, g.d_adj, &seg, 1, n, st));
   return GGB_OK;
 }
 
@@ -690,6 +696,7 @@ void ggb_finalize(void) {
   cudaSetDevice(g.device);
   if (g.stream) cudaStreamSynchronize(g.stream);
   cudaFree(g.d_adj);
+  cudaFree(g.d_adj16);
   cudaFree(g.d_adj2);
   cudaFree(g.d_rh);
   cudaFree(g.d_inv);
@@ -817,7 +824,7 @@ int ggb_eval_general_partial(int nodes, int based_nodes, int groups, int degree,
   if (rc) return rc;
   rc = ensure_ready(-1);
   if (rc) return rc;
-  rc = stage_adj(adj, (size_t)nodes * degree, g.stream);
+  rc = stage_adj(adj, (size_t)nodes * degree, nodes, g.stream);
   if (rc) return rc;
   rc = launch_apsp(g.d_adj, nodes, degree, based_nodes, based_nodes * groups, added_centers, groups,
                    rank, procs, g.stream);
@@ -945,7 +952,7 @@ int eval_grid_impl(int nodes, int degree, const int* deg, int groups, const int*
   if (rc) return rc;
   const size_t n = (size_t)nodes * degree;
   cudaStream_t st = g.stream;
-  rc = stage_adj(adj, n, st);
+  rc = stage_adj(adj, n, nodes, st);
   if (rc) return rc;
   if ((rc = grow_device(&g.d_adj2, &g.cap_adj2, n))) return rc;
   if ((rc = grow_device(&g.d_rh, &g.cap_rh, (size_t)nodes))) return rc;
@@ -1007,7 +1014,7 @@ int ggb_eval_general_nonregular(int nodes, int based_nodes, int groups, int max_
   if (rc) return rc;
   const size_t n = (size_t)nodes * max_degree;
   cudaStream_t st = g.stream;
-  rc = stage_adj(adj, n, st);
+  rc = stage_adj(adj, n, nodes, st);
   if (rc) return rc;
   if ((rc = grow_device(&g.d_adj2, &g.cap_adj2, n))) return rc;
   if ((rc = stage_deg(num_degrees, (size_t)nodes, st))) return rc;

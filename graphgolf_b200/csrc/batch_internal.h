@@ -2,6 +2,7 @@
 // enqueue batch evaluations (the batch API and the device annealing engine).
 // Not part of the public C ABI.
 #pragma once
+#include <cstdint>
 #include <cuda_runtime.h>
 
 #include <vector>
@@ -18,6 +19,7 @@ struct ggb_batch {
   long long adj_ints = 0;
   int* d_adj = nullptr;
   int* h_adj = nullptr;              // pinned staging for ggb_batch_eval
+  uint16_t* d_adj16 = nullptr;       // 16-bit ids on their way to d_adj (every N <= 65536)
   ggb::BatchGraph* d_graphs = nullptr;
   ggb::BatchOut* d_out = nullptr;
   ggb::BatchOut* h_out = nullptr;

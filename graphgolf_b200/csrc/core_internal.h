@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <cstddef>
+#include <cstdint>
 
 namespace ggb {
 
@@ -34,6 +35,13 @@ struct StageSeg {
 // buffer must not feed a copy still in flight.  Returns the first CUDA error.
 cudaError_t stage_upload(int device, int* pinned, int* dev, const StageSeg* segs, int nsegs, size_t total,
                          cudaStream_t st);
+
+// Like stage_upload(), but when dev16 is given and every int lies in
+// [0, 65535], sends the ids as 16-bit values into dev16 and widens them into
+// dev on the device (one kernel launch on st).  Otherwise sends the ints as
+// they are.  Either way dev ends up holding exactly the caller's ints.
+cudaError_t stage_upload_ids(int device, int* pinned, uint16_t* dev16, int* dev, const StageSeg* segs, int nsegs,
+                             size_t total, cudaStream_t st);
 
 // Number of threads stage_upload() copies with, the caller included.
 int stage_threads();

@@ -111,12 +111,15 @@ def test_bad_entry_reported_and_batch_reusable(gpu):
     sizes = [300, 400, 500]
     a = [graphs.random_regular(n, 4, n).adj for n in sizes]
     bad = [x.copy() for x in a]
-    bad[1][17, 2] = 400   # == nodes of graph 1: out of range
     with gg.Batch(sizes, 4) as b:
-        with pytest.raises(gg.EvaluationError) as ei:
-            b.evaluate(bad)
-        assert ei.value.code == -3 and "graph 1" in str(ei.value)
-        assert [_got(r) for r in b.evaluate(a)] == [_want(x, 1) for x in a]
+        # 400 == nodes of graph 1 travels as a 16-bit id; 1 << 20 and -1 make
+        # the upload fall back to plain ints.  All are caught on the device.
+        for v in (400, 1 << 20, -1):
+            bad[1][17, 2] = v
+            with pytest.raises(gg.EvaluationError) as ei:
+                b.evaluate(bad)
+            assert ei.value.code == -3 and "graph 1" in str(ei.value), v
+            assert [_got(r) for r in b.evaluate(a)] == [_want(x, 1) for x in a]
 
 
 def test_bad_sizes_rejected(gpu):

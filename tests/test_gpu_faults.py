@@ -20,15 +20,36 @@ def _ok_after(lib):
 
 def test_adjacency_out_of_range(gpu):
     adj = graphs.random_regular(400, 6, 4).adj.copy()
-    adj[123, 2] = 400
-    with pytest.raises(gg.EvaluationError) as e:
-        gg.evaluate(adj)
-    assert e.value.code == -3
-    adj[123, 2] = -7
-    with pytest.raises(gg.EvaluationError) as e:
-        gg.evaluate(adj)
-    assert e.value.code == -3
-    _ok_after(gpu)
+    good = adj[123, 2]
+    # 400 and 65535 travel as 16-bit ids; the others make the upload fall back
+    # to plain ints.  Each is caught by the device bounds check, and the next
+    # upload of the valid graph is exact.
+    for bad in (400, -7, 65535, 65536, 70000, 1 << 30, -65536):
+        adj[123, 2] = bad
+        with pytest.raises(gg.EvaluationError) as e:
+            gg.evaluate(adj)
+        assert e.value.code == -3, bad
+        adj[123, 2] = good
+        r = gg.evaluate(adj)
+        assert (r.connected, r.diameter, r.aspl, r.total) == oracle.general(adj), bad
+
+
+def test_out_of_range_id_in_a_later_staging_unit(gpu):
+    """An upload of several staging units (N=40000, d=8: 320 000 ids) with
+    one id past 16 bits in the last unit: the narrowed units already sent are
+    dropped, the ints are sent as they are, and the device reports the id."""
+    adj = graphs.random_regular(40000, 8, 9).adj.copy()
+    r0 = gg.evaluate(adj)
+    assert (r0.connected, r0.diameter, r0.aspl, r0.total) == oracle.general(adj)
+    good = adj[39990, 5]
+    for bad in (40000, 65536, -2):
+        adj[39990, 5] = bad
+        with pytest.raises(gg.EvaluationError) as e:
+            gg.evaluate(adj)
+        assert e.value.code == -3, bad
+        adj[39990, 5] = good
+        r = gg.evaluate(adj)
+        assert (r.connected, r.diameter, r.aspl, r.total) == (r0.connected, r0.diameter, r0.aspl, r0.total)
 
 
 def test_rotate_hash_not_a_permutation(gpu):
