@@ -95,6 +95,7 @@ CORE_SIGNATURES = {
     "ggb_launch_general_partial_device": (_I, [_I, _I, _I, _I, _P, _I, _I, _I, _P]),
     "ggb_collect_partial": (_I, [_P, C.POINTER(ggb_partial)]),
     "ggb_kernel_launches": (_LL, []),
+    "ggb_h2d_bytes": (_LL, []),
     "ggb_trace_enable": (_I, [_I]),
     "ggb_set_timing": (_I, [_I]),
     "ggb_kernel_times": (_I, [C.POINTER(C.c_double), C.POINTER(C.c_double)]),

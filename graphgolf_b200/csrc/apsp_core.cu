@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cfloat>
 #include <climits>
 #include <cmath>
@@ -150,6 +151,7 @@ State g;
 std::mutex g_mu;
 char g_err[512] = "";
 long long g_launches = 0;
+std::atomic<long long> g_h2d{0};   // adjacency bytes sent host to device (staging threads add to it)
 
 int fail(int code, const char* fmt, ...) {
   va_list ap;
@@ -616,6 +618,8 @@ int core_fail(int code, const char* fmt, ...) {
 
 void core_add_launches(long long n) { g_launches += n; }
 
+void core_add_h2d(long long bytes) { g_h2d.fetch_add(bytes, std::memory_order_relaxed); }
+
 }  // namespace ggb
 
 namespace {
@@ -667,6 +671,8 @@ extern "C" {
 const char* ggb_version(void) { return "graphgolf_b200 0.1 (sm_100a)"; }
 const char* ggb_last_error(void) { return g_err; }
 long long ggb_kernel_launches(void) { return g_launches; }
+
+long long ggb_h2d_bytes(void) { return g_h2d.load(std::memory_order_relaxed); }
 
 int ggb_device_count(void) {
   int n = 0;

@@ -16,6 +16,9 @@ int core_fail(int code, const char* fmt, ...);
 // Adds n to the launch counter.
 void core_add_launches(long long n);
 
+// Adds to the count of adjacency bytes sent host to device (thread-safe).
+void core_add_h2d(long long bytes);
+
 // Copies n ints from pageable memory into pinned staging (non-temporal
 // stores where the CPU has AVX2, memcpy otherwise).
 void stage_copy(int* dst, const int* src, size_t n);

@@ -239,6 +239,7 @@ class Pool {
           const cudaError_t e = cudaMemcpyAsync(static_cast<uint16_t*>(dev_) + un.lo, h + un.lo,
                                                 (un.hi - un.lo) * sizeof(uint16_t), cudaMemcpyHostToDevice, stream_);
           if (e != cudaSuccess) fail(e);
+          ggb::core_add_h2d((long long)((un.hi - un.lo) * sizeof(uint16_t)));
         }
       } else {
         int* h = static_cast<int*>(pinned_);
@@ -250,6 +251,7 @@ class Pool {
           const cudaError_t e = cudaMemcpyAsync(static_cast<int*>(dev_) + un.lo, h + un.lo,
                                                 (un.hi - un.lo) * sizeof(int), cudaMemcpyHostToDevice, stream_);
           if (e != cudaSuccess) fail(e);
+          ggb::core_add_h2d((long long)((un.hi - un.lo) * sizeof(int)));
         }
       }
       done_.fetch_add(1, std::memory_order_acq_rel);

@@ -190,9 +190,15 @@ int ggb_launch_general_device(int nodes, int based_nodes, int groups, int degree
 /* Waits for the last launch on `stream` and returns its result. */
 int ggb_collect(void *stream, ggb_result *out);
 
-/* Number of this library's kernels enqueued since load (each evaluation is
- * one persistent kernel plus, for grids, two relabel kernels). */
+/* Number of this library's kernels enqueued since load: every kernel of an
+ * evaluation (ball pre-pass, persistent kernel, the grid relabel kernels, the
+ * widening of 16-bit ids after an upload) counts once per launch. */
 long long ggb_kernel_launches(void);
+
+/* Bytes of adjacency this library has copied from host to device since load:
+ * what the host-buffer entry points send over PCIe (2 bytes per id when the
+ * ids fit 16 bits, else 4). */
+long long ggb_h2d_bytes(void);
 
 /* ---- evaluation without device allocation ------------------------------- */
 
