@@ -161,6 +161,19 @@ double make_plan(ggb_batch* b, int R, int T, bool keep) {
     off += 2 * cells;
   }
   b->team_start[n_teams] = (int)b->team_list.size();
+  // Stamps pay where the stamping sweeps run: 4096-source windows, degree <= 16.
+  b->team_soff.assign(n_teams, 0);
+  b->stamp_ints = 0;
+  bool stamping = false;
+  for (int i = 0; i < b->n; ++i) stamping = stamping || (R == 32 && b->d[i] <= 16);
+  if (stamping) {
+    for (int t = 0; t < n_teams; ++t) {
+      int mx = 0;
+      for (int k = b->team_start[t]; k < b->team_start[t + 1]; ++k) mx = std::max(mx, b->N[b->team_list[k]]);
+      b->team_soff[t] = b->stamp_ints;
+      b->stamp_ints += (mx + 31) / 32 * 32;   // each slice on a 128-byte boundary
+    }
+  }
   return makespan;
 }
 
@@ -192,6 +205,18 @@ int upload_plan(ggb_batch* b) {
                         cudaMemcpyHostToDevice, b->stream));
   BCUDA(cudaMemcpyAsync(b->d_tcells, b->team_cells.data(), b->team_cells.size() * sizeof(long long),
                         cudaMemcpyHostToDevice, b->stream));
+  if (b->stamp_ints > 0) {
+    if ((size_t)b->stamp_ints > b->cap_stamps) {
+      if (b->d_stamps) cudaFree(b->d_stamps);
+      b->d_stamps = nullptr;
+      b->cap_stamps = 0;
+      int rc = dev_alloc(&b->d_stamps, (size_t)b->stamp_ints);
+      if (rc) return rc;
+      b->cap_stamps = (size_t)b->stamp_ints;
+    }
+    BCUDA(cudaMemcpyAsync(b->d_tsoff, b->team_soff.data(), b->team_soff.size() * sizeof(long long),
+                          cudaMemcpyHostToDevice, b->stream));
+  }
   BCUDA(cudaStreamSynchronize(b->stream));
   return GGB_OK;
 }
@@ -211,6 +236,8 @@ ggb::BatchArgs batch_args(const ggb_batch* b) {
   a.sticky = b->sticky;
   a.n_teams = b->n_teams;
   a.team_ctas = b->T;
+  a.stamps = b->stamp_ints > 0 ? b->d_stamps : nullptr;
+  a.team_soff = b->stamp_ints > 0 ? b->d_tsoff : nullptr;
   return a;
 }
 
@@ -220,6 +247,7 @@ ggb::BatchArgs batch_args(const ggb_batch* b) {
 int ggb::batch_enqueue(ggb_batch* b, cudaStream_t st) {
   BCUDA(cudaMemsetAsync(b->d_ctrl, 0, (size_t)b->n_teams * sizeof(ggb::ApspCtrl), st));
   BCUDA(cudaMemsetAsync(b->d_out, 0, (size_t)b->n * sizeof(ggb::BatchOut), st));
+  if (b->stamp_ints > 0) BCUDA(cudaMemsetAsync(b->d_stamps, 0, (size_t)b->stamp_ints * sizeof(unsigned), st));
   ggb::BatchArgs args = batch_args(b);
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(b->ctas);
@@ -327,6 +355,8 @@ void destroy(ggb_batch* b) {
   cudaFree(b->d_tlist);
   cudaFree(b->d_toff);
   cudaFree(b->d_tcells);
+  cudaFree(b->d_tsoff);
+  cudaFree(b->d_stamps);
   cudaFree(b->d_scratch);
   for (auto& e : b->ev)
     if (e) cudaEventDestroy(e);
@@ -396,6 +426,7 @@ int create(int n_graphs, const int* nodes, const int* based_nodes, const int* gr
   if ((rc = dev_alloc(&b->d_tlist, (size_t)n_graphs))) return rc;
   if ((rc = dev_alloc(&b->d_toff, mt))) return rc;
   if ((rc = dev_alloc(&b->d_tcells, mt))) return rc;
+  if ((rc = dev_alloc(&b->d_tsoff, mt))) return rc;
   BCUDA(cudaHostAlloc(&b->h_out, (size_t)n_graphs * sizeof(ggb::BatchOut), cudaHostAllocDefault));
   BCUDA(cudaHostAlloc(&b->h_ctrl, mt * sizeof(ggb::ApspCtrl), cudaHostAllocDefault));
   std::vector<ggb::BatchGraph> gs(n_graphs);

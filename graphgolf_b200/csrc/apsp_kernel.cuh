@@ -107,11 +107,14 @@ struct ApspArgs {
   // The skipping sweep runs once the gathered level is at least this full
   // (per mille of N * sources).
   int skip_permille = 900;
-  // Optional full-row stamps, one per vertex, zeroed before the launch
-  // (single-graph evaluations only): stamp = (window id << 8) | L records that
-  // the vertex's row of that window is full from level L on.  The sweeps that
-  // set and read them are described at sweep_stamped.
+  // Optional full-row stamps, one per vertex, zeroed before the launch:
+  // stamp = (window id << 8) | L records that the vertex's row of that window
+  // is full from level L on.  The window id is stamp_base + t + 1 for window
+  // t, unique among the windows that share the stamps in one launch (the
+  // batch kernel advances stamp_base from one graph of a team to the next).
+  // The sweeps that set and read them are described at sweep_stamped.
   unsigned* stamps = nullptr;
+  unsigned stamp_base = 0;
 };
 
 __device__ __forceinline__ unsigned long long globaltimer_ns() {
@@ -988,9 +991,10 @@ __device__ __forceinline__ bool eval_windows(const ApspArgs& a, int cta, int nct
       const uint4* cur;           // S_kk rows the next sweep gathers from
       uint4* nxt;                 // rows it writes
       bool own_count = false;     // the first sweep of a ball window also reports S_3
-      // full-row stamps: phase-1 windows of single-graph evaluations, id = t + 1
-      unsigned* const stamps = (phase == 1 && a.levels == nullptr && !STATS) ? a.stamps : nullptr;
-      const unsigned stamp_id = (unsigned)t + 1u;
+      // full-row stamps: phase-1 windows without level recording; ids keep to 24 bits
+      const unsigned stamp_id = a.stamp_base + (unsigned)t + 1u;
+      unsigned* const stamps =
+          (phase == 1 && a.levels == nullptr && !STATS && stamp_id < (1u << 24)) ? a.stamps : nullptr;
       // base builds: this window's level rows and counts (never with the ball pre-pass)
       uint4* const lev0 = a.levels ? a.levels + (size_t)t * (a.level_cap + 1) * N * R : nullptr;
       long long* const lcnt = a.levels ? a.level_counts + (size_t)t * (a.level_cap + 1) : nullptr;
@@ -1354,6 +1358,10 @@ struct BatchArgs {
   const int* stop;                // when non-null and *stop != 0 the launch does nothing
   int* sticky;                    // when non-null: receives the first team's error code (never cleared here)
   int n_teams, team_ctas;
+  // Optional full-row stamps, zeroed before the launch: team t uses
+  // stamps + team_soff[t], one per vertex of its largest graph.
+  unsigned* stamps = nullptr;
+  const long long* team_soff = nullptr;
 };
 
 template <int R>
@@ -1383,6 +1391,8 @@ __global__ void __launch_bounds__(kThreads, 1) apsp_batch_kernel(const BatchArgs
   a.level_counts = nullptr;
   a.win_levels = nullptr;
   a.level_cap = 0;
+  a.stamps = b.stamps ? b.stamps + b.team_soff[team] : nullptr;
+  a.stamp_base = 0;
   unsigned long long bar_target = 0;
   unsigned gl = 0;
   int ntrace = 0;
@@ -1415,6 +1425,9 @@ __global__ void __launch_bounds__(kThreads, 1) apsp_batch_kernel(const BatchArgs
       w->windows = o.windows;
       w->done = 1;
     }
+    // the next graph's windows take the stamp ids after this graph's
+    const int W = (gr.win_bits > 0 && gr.win_bits < 128 * R) ? gr.win_bits : 128 * R;
+    a.stamp_base += (unsigned)((gr.n_src + W - 1) / W);
   }
 }
 

@@ -35,6 +35,13 @@ struct ggb_batch {
   long long* d_tcells = nullptr;     // [max_teams]
   uint4* d_scratch = nullptr;
   size_t cap_scratch = 0;            // uint4
+  // full-row stamps of the plan (4096-source windows, some degree <= 16):
+  // team t's slice starts at team_soff[t]; stamp_ints == 0 when unused
+  std::vector<long long> team_soff;
+  long long stamp_ints = 0;
+  long long* d_tsoff = nullptr;      // [max_teams]
+  unsigned* d_stamps = nullptr;
+  size_t cap_stamps = 0;             // unsigned
   int occ[6] = {0, 0, 0, 0, 0, 0};   // co-resident batch CTAs per SM, per log2(R)
   int max_teams = 0;                 // largest CTA count of any plan
   long long timeout_ns = 2000000000LL;
