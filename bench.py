@@ -175,8 +175,21 @@ def l2_gather_roof(lib, n: int, d: int, window_bits: int):
     return g.value if lib.ggb_probe_l2_gather(n, d, window_bits, 20, C.byref(g)) == 0 and g.value > 0 else None
 
 
+_L2_STREAM = {}
+
+
+def l2_stream_roof(lib):
+    """The L2 streaming ceiling (ggb_probe_l2_stream over a 64 MiB
+    L2-resident buffer, the size of the headline's two window matrices) in
+    GB/s, measured once per process (None if the probe fails)."""
+    if "gbs" not in _L2_STREAM:
+        g = C.c_double(0)
+        _L2_STREAM["gbs"] = g.value if lib.ggb_probe_l2_stream(64, 10, C.byref(g)) == 0 and g.value > 0 else None
+    return _L2_STREAM["gbs"]
+
+
 def roofline(kernel: str, alg: float, ms: float, l2_roof, hbm_peak: float, hbm_kind: str, traffic, lts,
-             lts_pct=None) -> dict:
+             lts_pct=None, l2_stream=None) -> dict:
     """Roofline of one kernel launch.  The sweeps' working set is L2-resident
     by design, so the bound is the L2 random-row gather rate measured live by
     the probe; the physical DRAM traffic (from the committed ncu capture) is
@@ -196,8 +209,15 @@ def roofline(kernel: str, alg: float, ms: float, l2_roof, hbm_peak: float, hbm_k
     if lts:
         out["lts_bytes_per_launch"] = lts
         out["lts_gbs"] = lts / (ms / 1e3) / 1e9
+        if l2_stream:
+            out["frac_of_l2_stream"] = out["lts_gbs"] / l2_stream
     if lts_pct is not None:
         out["lts_throughput_pct"] = lts_pct
+    if l2_stream:
+        out["l2_stream_gbs"] = l2_stream
+        out["l2_stream_source"] = ("ggb_probe_l2_stream: bulk copies of a 64 MiB L2-resident buffer into shared "
+                                   "memory, one CTA per SM, measured in this run (the L2 delivery ceiling; "
+                                   "frac_of_l2_stream compares the kernel's physical L2 bytes with it)")
     out["note"] = ("traffic = DRAM bytes per launch from the committed ncu capture under profiles/; "
                    "achieved counts every gather of every dense sweep, including the lanes the last-level "
                    "skip leaves out")
@@ -539,7 +559,8 @@ def main() -> int:
                     "levels": first.levels, "dense_levels": first.dense_levels,
                     "diameter": first.diameter, "total": first.total, "aspl": first.aspl},
             "roofline": roofline(f"apsp_persistent_kernel<{first.window_bits // 128}>", alg, pers_ms, l2_roof,
-                                 peak, peak_kind, traffic, lts, kp.get("lts_throughput_pct")),
+                                 peak, peak_kind, traffic, lts, kp.get("lts_throughput_pct"),
+                                 l2_stream_roof(lib)),
             "ball_prepass": {"ms_per_launch": ball_ms,
                              "algorithmic_bytes_per_launch": ball_bytes(n, d, first.windows, first.window_bits)
                              if ball_ms else 0,
@@ -795,10 +816,37 @@ def sa_bench(plain_steps: int) -> dict:
     if hill["learned"]["reached"] and hill["batched"]["reached"]:
         hill["network_gain"] = hill["batched"]["wall_s"] / hill["learned"]["wall_s"]
     out["hill_climbing"] = hill
+    out["filter_forward"] = filter_forward_block()
     ref = reference_sa_time(g, 100, t_max, t_min)
     if ref and "s_per_step" in ref:
         ref["extrapolated_plain_steps_s"] = ref["s_per_step"] * plain_steps
     out["reference_cpu_sa"] = ref
+    return out
+
+
+def filter_forward_block(rows: int = 4096, reps: int = 200) -> dict:
+    """The filter network's inference forward over one step's proposals
+    (4096 rows, 32 -> 256 -> 256 -> 1), device-timed with CUDA events over
+    back-to-back launches, against the measured dense BF16 tensor peak."""
+    import numpy as np
+    import graphgolf_b200 as gg
+    net = gg.FilterNet(rows, 1)
+    try:
+        x = np.random.default_rng(3).uniform(-1, 1, (rows, 32)).astype(np.float32)
+        ms = net.time_forward(x, reps)
+    finally:
+        net.close()
+    flops = 2.0 * rows * (32 * 256 + 256 * 256 + 256)
+    out = {"kernel": "forward_tc_kernel", "rows": rows, "ms_per_launch": ms, "flops_per_launch": flops,
+           "tflops": flops / (ms / 1e3) / 1e12}
+    try:
+        pk = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+        out["peak_tflops"] = pk["bf16_tflops"]
+        out["peak_source"] = "measured bf16_tflops (MEASURED_PEAKS.json)"
+    except (OSError, KeyError, ValueError):
+        out["peak_tflops"] = 1590.0
+        out["peak_source"] = "fallback 1.59 PFLOP/s"
+    out["frac"] = out["tflops"] / out["peak_tflops"]
     return out
 
 

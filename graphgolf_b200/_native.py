@@ -100,6 +100,7 @@ CORE_SIGNATURES = {
     "ggb_set_timing": (_I, [_I]),
     "ggb_kernel_times": (_I, [C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "ggb_probe_l2_gather": (_I, [_I, _I, _I, _I, C.POINTER(C.c_double)]),
+    "ggb_probe_l2_stream": (_I, [_I, _I, C.POINTER(C.c_double)]),
     "ggb_trace_read": (_I, [_P, _I]),
     "ggb_eval_general_partial": (_I, [_I, _I, _I, _I, _P, _I, _I, _I, C.POINTER(ggb_partial)]),
     "ggb_finish_general": (_I, [_I, C.POINTER(ggb_partial), C.POINTER(ggb_result)]),
@@ -125,6 +126,7 @@ CORE_SIGNATURES = {
     "ggb_mlp_get_params": (_I, [_P, _P]),
     "ggb_mlp_set_adam": (_I, [_P, C.c_float, C.c_float, C.c_float, C.c_float]),
     "ggb_mlp_forward_host": (_I, [_P, _P, _I, _P]),
+    "ggb_mlp_time_forward": (_I, [_P, _P, _I, _I, C.POINTER(C.c_double)]),
     "ggb_mlp_grads_host": (_I, [_P, _P, _P, _I, _P, _P]),
     "ggb_mlp_train_host": (_I, [_P, _P, _P, _I, _I, _P]),
     "ggb_sa_create": (_I, [_I, _I, _P, _I, _I, _I, C.c_ulonglong, C.POINTER(_P)]),
@@ -138,6 +140,11 @@ CORE_SIGNATURES = {
     "ggb_sa_run": (_I, [_P, _LL, C.POINTER(ggb_sa_stats)]),
     "ggb_sa_edges": (_I, [_P, _I, _P]),
     "ggb_sa_profile": (_I, [_P, _P]),
+    "ggb_sa_checkpoint_bytes": (_LL, [_P]),
+    "ggb_sa_save": (_I, [_P, _P, _LL]),
+    "ggb_sa_restore": (_I, [_P, _P, _LL]),
+    "ggb_sa_checkpoint_info": (_I, [_P, _LL, _IP, _IP, _IP, _IP]),
+    "ggb_sa_checkpoint_edges": (_I, [_P, _LL, _I, _P]),
     "ggb_sa_last_step": (_I, [_P, _P, _P]),
     "ggb_sa_check_delta": (_I, [_P, _IP, _IP, _IP, _IP]),
 }

@@ -129,11 +129,36 @@ class Annealer:
         _raise(self._lib.ggb_sa_check_delta(self._h, C.byref(c), C.byref(m), C.byref(u), C.byref(dn)))
         return (c.value, m.value, u.value, dn.value) if with_dense else (c.value, m.value, u.value)
 
+    def save(self) -> bytes:
+        """A checkpoint of the run: graph, best graph, step, schedule,
+        counters and (with a filter) the network's training state."""
+        n = int(self._lib.ggb_sa_checkpoint_bytes(self._h))
+        buf = C.create_string_buffer(n)
+        _raise(self._lib.ggb_sa_save(self._h, buf, n))
+        return buf.raw
+
+    def restore(self, ckpt: bytes) -> None:
+        """Continues the run saved in `ckpt`.  The annealer must have been
+        created from ``checkpoint_graph(ckpt)`` with the same arguments."""
+        _raise(self._lib.ggb_sa_restore(self._h, ckpt, len(ckpt)))
+
     def profile(self) -> np.ndarray:
         """[nodes][32]: entry [v][k] = vertices farther than k from v."""
         out = np.empty((self.nodes, 32), dtype=np.uint32)
         _raise(self._lib.ggb_sa_profile(self._h, out.ctypes.data))
         return out
+
+
+def checkpoint_graph(ckpt: bytes, best: bool = False) -> Graph:
+    """The current (or best) graph of an annealing checkpoint, to create the
+    annealer that ``Annealer.restore`` continues."""
+    from .graphs import create_adj
+    lib = load()
+    n, d, g, lines = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+    _raise(lib.ggb_sa_checkpoint_info(ckpt, len(ckpt), C.byref(n), C.byref(d), C.byref(g), C.byref(lines)))
+    e = np.empty((lines.value, 2), dtype=np.int32)
+    _raise(lib.ggb_sa_checkpoint_edges(ckpt, len(ckpt), 1 if best else 0, e.ctypes.data))
+    return Graph(n.value, d.value, e, create_adj(n.value, d.value, e), groups=g.value)
 
 
 class FilterNet:
@@ -181,6 +206,14 @@ class FilterNet:
         y = np.empty(a.shape[0], dtype=np.float32)
         _raise(self._lib.ggb_mlp_forward_host(self._h, a.ctypes.data, a.shape[0], y.ctypes.data))
         return y
+
+    def time_forward(self, x, reps: int = 50) -> float:
+        """Mean device time (ms) of one inference forward over the rows of x,
+        timed with CUDA events over `reps` back-to-back launches."""
+        a = np.ascontiguousarray(x, dtype=np.float32)
+        ms = C.c_double()
+        _raise(self._lib.ggb_mlp_time_forward(self._h, a.ctypes.data, a.shape[0], reps, C.byref(ms)))
+        return ms.value
 
     def grads(self, x, t) -> tuple[float, np.ndarray]:
         a = np.ascontiguousarray(x, dtype=np.float32)

@@ -8,7 +8,9 @@
 // matrix of the same shape, with the same 32-byte accesses, one launch per
 // sweep, at two CTAs per SM -- on buffers it allocates itself, and reports
 // the sweep's algorithmic bytes per second.  bench.py uses it as the roof of
-// its roofline report.
+// its roofline report.  ggb_probe_l2_stream measures the ceiling above it:
+// the rate at which L2 delivers an L2-resident buffer to the SMs, with bulk
+// copies that keep far more bytes in flight than registers can.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -111,7 +113,128 @@ float time_sweeps(uint4* a, uint4* b, const int* adj, int N, int d, int iters, u
   return ms / iters;
 }
 
+// ---- the L2 streaming roof ----------------------------------------------------
+// One CTA per SM, one thread driving a ring of kStreamStages shared-memory
+// stages: each stage receives a kStreamChunk-byte cp.async.bulk copy of the
+// L2-resident buffer and is refilled as soon as its mbarrier completes, so
+// about 192 KB per SM are in flight without any register holding them.  The
+// data are not read by the threads: the probe measures how fast L2 delivers
+// bytes to the SMs, the ceiling every L2-resident kernel runs under.  Every
+// wait is bounded (2 s by %globaltimer); one that runs out sets *err and the
+// remaining stages are drained with the same bound.
+constexpr int kStreamStages = 6;
+constexpr unsigned kStreamChunk = 32768;
+
+__device__ __forceinline__ bool stream_wait(unsigned bar, unsigned parity) {
+  unsigned long long t0 = 0;
+  for (;;) {
+    unsigned ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (ok) return true;
+    const unsigned long long t = ggb::globaltimer_ns();
+    if (t0 == 0) t0 = t;
+    else if (t - t0 > 2000000000ULL) return false;
+  }
+}
+
+__global__ void __launch_bounds__(32, 1) probe_stream_kernel(const unsigned char* __restrict__ src, long long chunks,
+                                                            int passes, int* err) {
+  extern __shared__ __align__(128) unsigned char ring[];
+  __shared__ alignas(8) unsigned long long bars[kStreamStages];
+  if (threadIdx.x != 0) return;
+  for (int s = 0; s < kStreamStages; ++s) {
+    const unsigned b = (unsigned)__cvta_generic_to_shared(&bars[s]);
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(b) : "memory");
+  }
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  const long long per = chunks > blockIdx.x ? (chunks - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
+  const long long total = per * passes;
+  bool ok = true;
+  long long i = 0;
+  for (; i < total; ++i) {
+    const int s = (int)(i % kStreamStages);
+    const unsigned b = (unsigned)__cvta_generic_to_shared(&bars[s]);
+    const long long use = i / kStreamStages;
+    if (use > 0 && !(ok = stream_wait(b, (unsigned)((use - 1) & 1)))) break;
+    const long long c = blockIdx.x + (i % per) * (long long)gridDim.x;
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(kStreamChunk) : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     (unsigned)__cvta_generic_to_shared(ring + (size_t)s * kStreamChunk)),
+                 "l"(src + c * (long long)kStreamChunk), "r"(kStreamChunk), "r"(b)
+                 : "memory");
+  }
+  // drain: the last use of every stage that was issued
+  for (int s = 0; s < kStreamStages; ++s) {
+    const long long uses = i > s ? (i - s + kStreamStages - 1) / kStreamStages : 0;
+    if (uses == 0) continue;
+    const unsigned b = (unsigned)__cvta_generic_to_shared(&bars[s]);
+    if (!stream_wait(b, (unsigned)((uses - 1) & 1))) ok = false;
+  }
+  if (!ok) atomicExch(err, 1);
+}
+
 }  // namespace
+
+// GB/s at which L2 delivers an L2-resident buffer of `mib` MiB (at most 96)
+// to the SMs: bulk copies into shared memory, one CTA per SM, averaged over
+// `iters` launches of 16 passes each after one warm-up launch.  No
+// counterpart in the reference; the streaming ceiling beside the gather roof.
+extern "C" int ggb_probe_l2_stream(int mib, int iters, double* gbs) {
+  if (mib <= 0 || mib > 96 || iters <= 0 || !gbs) return GGB_EINVAL;
+  int dev = 0, sms = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+    cudaGetLastError();
+    return GGB_ECUDA;
+  }
+  const size_t smem = (size_t)kStreamStages * kStreamChunk;
+  if (cudaFuncSetAttribute((const void*)probe_stream_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+      cudaSuccess) {
+    cudaGetLastError();
+    return GGB_ECUDA;
+  }
+  const long long chunks = (long long)mib * (1 << 20) / kStreamChunk;
+  unsigned char* buf = nullptr;
+  int* err = nullptr;
+  if (cudaMalloc(&buf, (size_t)chunks * kStreamChunk) != cudaSuccess || cudaMalloc(&err, sizeof(int)) != cudaSuccess) {
+    cudaGetLastError();
+    cudaFree(buf);
+    cudaFree(err);
+    return GGB_ENOMEM;
+  }
+  cudaMemset(buf, 0x5a, (size_t)chunks * kStreamChunk);
+  cudaMemset(err, 0, sizeof(int));
+  constexpr int kPasses = 16;   // 1 GiB a launch at 64 MiB, so the launch gaps stay small
+  probe_stream_kernel<<<sms, 32, smem>>>(buf, chunks, kPasses, err);
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0);
+  for (int it = 0; it < iters; ++it) probe_stream_kernel<<<sms, 32, smem>>>(buf, chunks, kPasses, err);
+  cudaEventRecord(e1);
+  cudaError_t e = cudaEventSynchronize(e1);
+  float ms = 0.f;
+  if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+  int h_err = 0;
+  if (e == cudaSuccess) e = cudaMemcpy(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(buf);
+  cudaFree(err);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return GGB_ECUDA;
+  }
+  if (h_err) return GGB_ETIMEOUT;
+  if (ms <= 0.f) return GGB_ECUDA;
+  *gbs = (double)chunks * kStreamChunk * kPasses * iters / (ms * 1e-3) / 1e9;
+  return GGB_OK;
+}
 
 // GB/s of random-row OR sweeps over an N x (window_bits/8)-byte matrix with d
 // random neighbours per row (a fixed-seed LCG graph), averaged over `iters`

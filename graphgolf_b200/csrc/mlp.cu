@@ -14,14 +14,15 @@
 // gradients are FP32.
 //
 // The inference forward that ranks the proposals (4096 rows a step) is one
-// fused kernel, forward_fused_kernel: weights staged in shared memory,
-// ldmatrix-fed mma.sync.m16n8k16, both layers and the output head without a
-// round trip through memory.  The training products (at most 256 rows) are
-// one warp per 16 x 8 output tile issuing mma.sync.m16n8k16 (BF16 in, FP32
-// accumulate) on operands read straight from L2.  At these sizes (0.5 GFLOP
-// a forward pass, tiles of 32 rows) the tcgen05/TMEM pipeline's set-up --
-// TMEM allocation, descriptors, an mbarrier round trip per tile -- would not
-// pay.
+// kernel on the fifth-generation tensor cores, forward_tc_kernel: per 128
+// rows, tcgen05.mma with both layers' FP32 accumulators in tensor memory,
+// operands staged in shared memory by bulk copies, bias, ReLU and the output
+// head applied between tcgen05.ld and the next product, no round trip through
+// global memory.  It replaced an mma.sync kernel of the same fusion (ldmatrix
+// fragments, 32 rows a CTA): 8.2 us against 10.3 us for 4096 rows.  The
+// training products (at most 256 rows, with the pre-activations the backward
+// needs) are one warp per 16 x 8 output tile issuing mma.sync.m16n8k16 (BF16
+// in, FP32 accumulate) on operands read straight from L2.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -121,37 +122,6 @@ __global__ void __launch_bounds__(128) gemm_tn_kernel(int M, int N, int K, const
   }
 }
 
-// ---- the fused inference forward ---------------------------------------------------
-// y = w3 . relu(W2 relu(W1 x + b1) + b2) + b3 for kFuseRows rows a CTA, in one
-// launch.  The CTA stages both weight matrices (BF16) and its rows of x in
-// shared memory with one cp.async.bulk copy per row, all completing on one
-// mbarrier, each row padded by 16 bytes so that the eight 16-byte rows an
-// ldmatrix reads fall in eight different bank groups;
-// ldmatrix.x4 feeds mma.sync.m16n8k16 (BF16 in, FP32 accumulate); the first
-// hidden layer goes back to shared memory as BF16 after bias and ReLU, the
-// second is never stored: each lane applies bias, ReLU and w3 to its
-// accumulators and the row sums meet in shared memory.  Numerics as the
-// unfused path (BF16 operands, FP32 accumulation, H1 rounded to BF16); only
-// the summation order of the output dot product differs.  8 warps: warp w
-// owns rows 16 (w % 2) .. +16 and output columns 64 (w / 2) .. +64.  With
-// 64 rows and 16 warps a CTA, tensor-pipe activity rose from 16 % to 26 % of
-// active cycles, but the 4096-row pass took 12.3 us against 10.5 us: half as
-// many CTAs stage the weights.
-constexpr int kFuseRows = 32;
-constexpr int kFuseThreads = 32 * (kFuseRows / 16) * 4;   // a warp per (16-row tile, 64 columns)
-constexpr int kLdW2 = kHidden + 8;      // padded row of W2 / H1 (bf16 elements)
-constexpr int kLdW1 = kFeatures + 8;    // padded row of W1 / x
-constexpr size_t kFuseSmem = ((size_t)kHidden * kLdW2 + (size_t)kHidden * kLdW1 + (size_t)kFuseRows * kLdW1 +
-                              (size_t)kFuseRows * kLdW2) * sizeof(bf16) +
-                             (3 * (size_t)kHidden + (size_t)kFuseRows * 4) * sizeof(float);
-
-__device__ __forceinline__ void ldmatrix_x4(uint32_t (&r)[4], const bf16* p) {
-  const unsigned a = (unsigned)__cvta_generic_to_shared(p);
-  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];"
-               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
-               : "r"(a));
-}
-
 // Bulk copies global -> shared (cp.async.bulk, completion on an mbarrier).
 __device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
 __device__ __forceinline__ void bulk_copy(void* dst, const void* src, unsigned bytes, unsigned bar) {
@@ -177,138 +147,239 @@ __device__ __forceinline__ unsigned long long global_ns() {
   return t;
 }
 
-// acc[nt][4] += A (16 rows at a, row stride lda) * B^T (8 * NT rows at b, row
-// stride ldb) over K columns; A and B^T are [.][K] BF16 in shared memory.
-template <int NT, int K>
-__device__ __forceinline__ void warp_mma_tile(float (&acc)[NT][4], const bf16* a, int lda, const bf16* b, int ldb) {
-  const int lane = threadIdx.x & 31;
-  const int ar = lane & 15, ak = (lane >> 4) * 8;                 // A: rows 0-15, k halves
-  const int bn = (lane >> 4) * 8 + (lane & 7), bk = ((lane >> 3) & 1) * 8;   // B: two n-tiles, k halves
-  // unrolled: the next k-step's fragments load while this step's products issue
-#pragma unroll
-  for (int k0 = 0; k0 < K; k0 += 16) {
-    uint32_t af[4];
-    ldmatrix_x4(af, a + ar * lda + k0 + ak);
-#pragma unroll
-    for (int p = 0; p < NT / 2; ++p) {
-      uint32_t bf[4];
-      ldmatrix_x4(bf, b + (p * 16 + bn) * ldb + k0 + bk);
-      mma_16816(acc[2 * p], af[0], af[1], af[2], af[3], bf[0], bf[1]);
-      mma_16816(acc[2 * p + 1], af[0], af[1], af[2], af[3], bf[2], bf[3]);
-    }
-  }
+// ---- the tcgen05 inference forward ---------------------------------------------------
+// The same y = w3 . relu(W2 relu(W1 x + b1) + b2) + b3, on the fifth-generation
+// tensor cores: one CTA per 128 rows (M of one tcgen05.mma), both layers'
+// accumulators in tensor memory (TMEM), operands in shared memory.
+//   * Staging: W1 and W2 sit in global memory already in the operand layout
+//     (written by the cast and Adam kernels), so bulk copies bring them in:
+//     W1 (16 KB) on one mbarrier, W2 (8 x 16 KB) on another, so that layer 1
+//     and its epilogue run while W2 is still arriving; the CTA's rows of x are
+//     stored into the same layout by plain 16-byte stores.
+//   * Layer 1: two tcgen05.mma (M 128, N 256, K 16) into TMEM columns 0-255.
+//   * Epilogue 1: warp w reads TMEM lanes 32 (w % 4) .. +32 (its rows) and
+//     columns 128 (w / 4) .. +128 with tcgen05.ld, adds b1, applies ReLU,
+//     rounds to BF16 and stores H1 in the operand layout.
+//   * Layer 2: sixteen tcgen05.mma (K 16 each) into columns 256-511.
+//   * Epilogue 2: bias, ReLU and the w3 dot product per thread (a thread owns
+//     a row), the two column halves added in shared memory.
+// One thread issues the MMAs; tcgen05.commit arrives on an mbarrier that the
+// CTA waits on (bounded by %globaltimer, 2 s; a wait that runs out leaves
+// NaN for the CTA's rows).  Numerics as the other forwards: BF16 operands,
+// FP32 accumulation, H1 rounded to BF16.
+namespace tc {
+constexpr int kRows = 128;
+constexpr int kThreads = 256;
+constexpr uint32_t kW2Bytes = kHidden * kHidden * 2;      // 131072
+constexpr uint32_t kW1Bytes = kHidden * kFeatures * 2;    // 16384
+constexpr uint32_t kXBytes = kRows * kFeatures * 2;       // 8192
+constexpr uint32_t kH1Bytes = kRows * kHidden * 2;        // 65536
+constexpr uint32_t kSOffW1 = kW2Bytes;
+constexpr uint32_t kSOffX = kSOffW1 + kW1Bytes;
+constexpr uint32_t kSOffH1 = kSOffX + kXBytes;
+constexpr uint32_t kSOffVec = kSOffH1 + kH1Bytes;          // b1, b2, w3 (FP32)
+constexpr uint32_t kSOffPart = kSOffVec + 3 * kHidden * 4; // [kRows][2] FP32
+constexpr size_t kSmem = kSOffPart + kRows * 2 * 4;
+constexpr uint32_t kTmemCols = 512;                       // layer 1: 0-255, layer 2: 256-511
+// Instruction descriptor of kind::f16: FP32 accumulator (bits 4-5 = 1), A and
+// B BF16 (bits 7-9 = 1, 10-12 = 1), both K-major (bits 15, 16 = 0), N >> 3
+// in bits 17-22, M >> 4 in bits 24-28.
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kHidden >> 3) << 17) |
+                            ((uint32_t)(kRows >> 4) << 24);
+static_assert(kSmem + 1024 <= 227 * 1024, "the operands and the static barriers must fit one CTA's shared memory");
+}  // namespace tc
+
+// Element offset of (row r, column k) of a [rows][K] BF16 operand in the
+// K-major, no-swizzle layout: 8 x 8 core matrices of 128 contiguous bytes,
+// core (r / 8, k / 8) at byte (r / 8) * 16 K + (k / 8) * 128.  Descriptor:
+// leading-dimension offset 128 bytes (next 8 columns), stride offset 16 K
+// bytes (next 8 rows).
+__host__ __device__ constexpr int umma_k_off(int r, int k, int K) {
+  return (r >> 3) * (K * 8) + (k >> 3) * 64 + (r & 7) * 8 + (k & 7);
 }
 
-__global__ void __launch_bounds__(kFuseThreads) forward_fused_kernel(const bf16* __restrict__ X, int rows,
-                                                                      const bf16* __restrict__ W1b,
-                                                                      const bf16* __restrict__ W2b,
-                                                                      const float* __restrict__ params,
-                                                                      float* __restrict__ y) {
-  extern __shared__ uint4 s_fuse[];
-  bf16* const W2s = reinterpret_cast<bf16*>(s_fuse);
-  bf16* const W1s = W2s + kHidden * kLdW2;
-  bf16* const Xs = W1s + kHidden * kLdW1;
-  bf16* const H1s = Xs + kFuseRows * kLdW1;
-  float* const b1s = reinterpret_cast<float*>(H1s + kFuseRows * kLdW2);
+// Shared-memory matrix descriptor: start, leading and stride byte offsets in
+// 16-byte units, descriptor version 1 (bits 46-47), no swizzle (bits 61-63 = 0).
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accum) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+      ::"r"(d_tmem), "l"(a), "l"(b), "r"(idesc), "r"(accum)
+      : "memory");
+}
+__device__ __forceinline__ void umma_commit(unsigned bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// 32 consecutive FP32 columns of this thread's TMEM lane.
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n\t"
+      "tcgen05.wait::ld.sync.aligned;"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+        "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+        "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+        "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+      : "r"(taddr)
+      : "memory");
+}
+
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned bar, unsigned parity) {
+  if (mbar_try_wait_parity(bar, parity)) return true;
+  const unsigned long long t0 = global_ns();
+  while (!mbar_try_wait_parity(bar, parity))
+    if (global_ns() - t0 > 2000000000ULL) return false;
+  return true;
+}
+
+__global__ void __launch_bounds__(tc::kThreads, 1) forward_tc_kernel(const bf16* __restrict__ X, int rows,
+                                                                   const bf16* __restrict__ W1u,
+                                                                   const bf16* __restrict__ W2u,
+                                                                   const float* __restrict__ params,
+                                                                   float* __restrict__ y) {
+  using namespace tc;
+  extern __shared__ __align__(1024) unsigned char s_tc[];
+  __shared__ alignas(8) unsigned long long s_bars[3];   // [0] W1 staged, [1] MMA completion, [2] W2 staged
+  __shared__ uint32_t s_tmem;
+  __shared__ int s_ok;
+  bf16* const W2s = reinterpret_cast<bf16*>(s_tc);
+  bf16* const W1s = reinterpret_cast<bf16*>(s_tc + kSOffW1);
+  bf16* const Xs = reinterpret_cast<bf16*>(s_tc + kSOffX);
+  bf16* const H1s = reinterpret_cast<bf16*>(s_tc + kSOffH1);
+  float* const b1s = reinterpret_cast<float*>(s_tc + kSOffVec);
   float* const b2s = b1s + kHidden;
   float* const w3s = b2s + kHidden;
-  float* const part = w3s + kHidden;   // [kFuseRows][4] partial output sums
-  __shared__ alignas(8) unsigned long long s_bar;
-  const int r0 = blockIdx.x * kFuseRows;
-  const int valid = min(kFuseRows, rows - r0);
-  // Staging: one bulk copy per matrix row (W2: 512 bytes, W1 and x: 64 bytes)
-  // into the padded rows, all in flight at once, completing on one mbarrier.
-  const unsigned bar = smem_u32(&s_bar);
-  if (threadIdx.x == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+  float* const part = reinterpret_cast<float*>(s_tc + kSOffPart);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int r0 = blockIdx.x * kRows;
+  const int valid = min(kRows, rows - r0);
+  const unsigned bar_st = smem_u32(&s_bars[0]), bar_mma = smem_u32(&s_bars[1]), bar_w2 = smem_u32(&s_bars[2]);
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_st) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_mma) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_w2) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    const unsigned bytes = (unsigned)(kHidden * (kHidden + kFeatures) + valid * kFeatures) * (unsigned)sizeof(bf16);
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
+                 "r"(kTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
   __syncthreads();
-  asm volatile("fence.proxy.async.global;" ::: "memory");
-  for (int i = threadIdx.x; i < kHidden; i += blockDim.x) {
-    bulk_copy(W2s + i * kLdW2, W2b + (long long)i * kHidden, kHidden * sizeof(bf16), bar);
-    bulk_copy(W1s + i * kLdW1, W1b + (long long)i * kFeatures, kFeatures * sizeof(bf16), bar);
+  if (tid == 0) {
+    // W1 first, on its own barrier: layer 1 and its epilogue run while W2 arrives
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_st), "r"(kW1Bytes) : "memory");
+    bulk_copy(W1s, W1u, kW1Bytes, bar_st);
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_w2), "r"(kW2Bytes) : "memory");
+    for (uint32_t c = 0; c < kW2Bytes; c += 16384u)
+      bulk_copy(s_tc + c, reinterpret_cast<const unsigned char*>(W2u) + c, 16384u, bar_w2);
   }
-  for (int i = threadIdx.x; i < kFuseRows; i += blockDim.x) {
-    if (i < valid) {
-      bulk_copy(Xs + i * kLdW1, X + (long long)(r0 + i) * kFeatures, kFeatures * sizeof(bf16), bar);
-    } else {
-      for (int c = 0; c < kFeatures; c += 8) *reinterpret_cast<uint4*>(Xs + i * kLdW1 + c) = make_uint4(0u, 0u, 0u, 0u);
-    }
+  // this CTA's rows of x (zeros past the last row) into the operand layout
+  for (int i = tid; i < kRows * (kFeatures / 8); i += kThreads) {
+    const int r = i / (kFeatures / 8), c = (i % (kFeatures / 8)) * 8;
+    uint4 v = make_uint4(0u, 0u, 0u, 0u);
+    if (r < valid) v = *reinterpret_cast<const uint4*>(X + (long long)(r0 + r) * kFeatures + c);
+    *reinterpret_cast<uint4*>(Xs + umma_k_off(r, c, kFeatures)) = v;
   }
-  for (int i = threadIdx.x; i < kHidden; i += blockDim.x) {
+  for (int i = tid; i < kHidden; i += kThreads) {
     b1s[i] = params[kOffB1 + i];
     b2s[i] = params[kOffB2 + i];
     w3s[i] = params[kOffW3 + i];
   }
-  // bounded wait (2 s); a wait that runs out leaves NaN for this CTA's rows
-  bool staged = mbar_try_wait_parity(bar, 0u);
-  if (!staged) {
-    const unsigned long long t0 = global_ns();
-    while (!(staged = mbar_try_wait_parity(bar, 0u)))
-      if (global_ns() - t0 > 2000000000ULL) break;
+  // the generic-proxy stores of x must be visible to the tensor cores' reads
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = s_tmem;
+  if (tid == 0) {
+    const bool staged = mbar_wait_bounded(bar_st, 0u);
+    if (staged) {
+      tc_fence_after();
+#pragma unroll
+      for (int ks = 0; ks < kFeatures / 16; ++ks)
+        umma_bf16(tmem, umma_desc(smem_u32(Xs) + 256u * ks, 128u, 16u * kFeatures),
+                  umma_desc(smem_u32(W1s) + 256u * ks, 128u, 16u * kFeatures), kIdesc, ks > 0);
+      umma_commit(bar_mma);
+    }
+    s_ok = staged;
   }
   __syncthreads();
-  if (__syncthreads_or(!staged)) {
-    if (threadIdx.x < valid) y[r0 + threadIdx.x] = __int_as_float(0x7fc00000);
-    return;
-  }
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  constexpr int kRowTiles = kFuseRows / 16;
-  const int mrow = (warp % kRowTiles) * 16, ncol = (warp / kRowTiles) * 64;
-  const int g = lane >> 2, t = lane & 3;
-  // layer 1: H1 = relu(x W1^T + b1), K = 32
-  {
-    float acc[8][4];
+  const bool ok1 = s_ok && mbar_wait_bounded(bar_mma, 0u);
+  const int q = warp & 3, h = warp >> 2;
+  const int row = 32 * q + lane;
+  const uint32_t lane_base = tmem + ((uint32_t)(32 * q) << 16);
+  bool failed = __syncthreads_or(!ok1);
+  if (!failed) {
+    tc_fence_after();
+    // epilogue 1: H1 = bf16(relu(acc + b1)) into the operand layout
+#pragma unroll 1
+    for (int j = 0; j < 4; ++j) {
+      const int col0 = 128 * h + 32 * j;
+      uint32_t v[32];
+      tmem_ld32(lane_base + (uint32_t)col0, v);
 #pragma unroll
-    for (int i = 0; i < 8; ++i) acc[i][0] = acc[i][1] = acc[i][2] = acc[i][3] = 0.f;
-    warp_mma_tile<8, kFeatures>(acc, Xs + mrow * kLdW1, kLdW1, W1s + ncol * kLdW1, kLdW1);
+      for (int m = 0; m < 4; ++m) {
+        uint32_t pk[4];
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      const int n = ncol + i * 8 + 2 * t;
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int m = mrow + g + (q >= 2 ? 8 : 0), nn = n + (q & 1);
-        const float v = acc[i][q] + b1s[nn];
-        H1s[m * kLdW2 + nn] = __float2bfloat16_rn(v > 0.f ? v : 0.f);
+        for (int e = 0; e < 4; ++e) {
+          const int c = col0 + 8 * m + 2 * e;
+          const float f0 = fmaxf(__uint_as_float(v[8 * m + 2 * e]) + b1s[c], 0.f);
+          const float f1 = fmaxf(__uint_as_float(v[8 * m + 2 * e + 1]) + b1s[c + 1], 0.f);
+          const __nv_bfloat162 b2v = __floats2bfloat162_rn(f0, f1);
+          pk[e] = *reinterpret_cast<const uint32_t*>(&b2v);
+        }
+        *reinterpret_cast<uint4*>(H1s + umma_k_off(row, col0 + 8 * m, kHidden)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
       }
     }
+    bool w2_ok = true;
+    if (tid == 0) w2_ok = mbar_wait_bounded(bar_w2, 0u);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    tc_fence_before();
+    failed = __syncthreads_or(!w2_ok);
   }
-  __syncthreads();
-  // layer 2 and the head: y = w3 . relu(H1 W2^T + b2) + b3, K = 256
-  float acc[8][4];
+  if (!failed) {
+    if (tid == 0) {
+      tc_fence_after();
 #pragma unroll
-  for (int i = 0; i < 8; ++i) acc[i][0] = acc[i][1] = acc[i][2] = acc[i][3] = 0.f;
-  warp_mma_tile<8, kHidden>(acc, H1s + mrow * kLdW2, kLdW2, W2s + ncol * kLdW2, kLdW2);
-  float s_lo = 0.f, s_hi = 0.f;   // rows mrow + g and mrow + g + 8
+      for (int ks = 0; ks < kHidden / 16; ++ks)
+        umma_bf16(tmem + (uint32_t)kHidden, umma_desc(smem_u32(H1s) + 256u * ks, 128u, 16u * kHidden),
+                  umma_desc(smem_u32(W2s) + 256u * ks, 128u, 16u * kHidden), kIdesc, ks > 0);
+      umma_commit(bar_mma);
+    }
+    const bool ok2 = mbar_wait_bounded(bar_mma, 1u);
+    failed = __syncthreads_or(!ok2);
+    if (!failed) {
+      tc_fence_after();
+      // epilogue 2: this thread's row, columns 128 h .. +128
+      float s = 0.f;
+#pragma unroll 1
+      for (int j = 0; j < 4; ++j) {
+        const int col0 = 128 * h + 32 * j;
+        uint32_t v[32];
+        tmem_ld32(lane_base + (uint32_t)(kHidden + col0), v);
 #pragma unroll
-  for (int i = 0; i < 8; ++i) {
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const int nn = ncol + i * 8 + 2 * t + (q & 1);
-      float v = acc[i][q] + b2s[nn];
-      v = (v > 0.f ? v : 0.f) * w3s[nn];
-      if (q < 2) s_lo += v; else s_hi += v;
+        for (int e = 0; e < 32; ++e) s = fmaf(fmaxf(__uint_as_float(v[e]) + b2s[col0 + e], 0.f), w3s[col0 + e], s);
+      }
+      part[row * 2 + h] = s;
     }
   }
-#pragma unroll
-  for (int o = 1; o < 4; o <<= 1) {
-    s_lo += __shfl_xor_sync(0xffffffffu, s_lo, o);
-    s_hi += __shfl_xor_sync(0xffffffffu, s_hi, o);
-  }
-  if (t == 0) {
-    part[(mrow + g) * 4 + ncol / 64] = s_lo;
-    part[(mrow + g + 8) * 4 + ncol / 64] = s_hi;
-  }
+  tc_fence_before();
   __syncthreads();
-  if (threadIdx.x < valid) {
-    const float* pr = part + threadIdx.x * 4;
-    y[r0 + threadIdx.x] = ((pr[0] + pr[1]) + (pr[2] + pr[3])) + params[kOffB3];
+  if (tid < valid) y[r0 + tid] = failed ? __int_as_float(0x7fc00000) : (part[2 * tid] + part[2 * tid + 1]) + params[kOffB3];
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
   }
 }
 
@@ -382,13 +453,31 @@ __global__ void col_sum_kernel(const float* __restrict__ in, int rows, int cols,
   out[c] = s;
 }
 
+// The BF16 copies of parameter i (value v) that the products read: W1 and
+// W2 row-major, W2 transposed, and W1 / W2 in the tcgen05 operand layout.
+__device__ __forceinline__ void store_bf16_copies(int i, float v, bf16* __restrict__ w1b, bf16* __restrict__ w2b,
+                                                  bf16* __restrict__ w2tb, bf16* __restrict__ w1u,
+                                                  bf16* __restrict__ w2u) {
+  const bf16 b = __float2bfloat16_rn(v);
+  if (i < kOffB1) {
+    w1b[i] = b;
+    w1u[umma_k_off(i / kFeatures, i % kFeatures, kFeatures)] = b;
+  } else if (i >= kOffW2 && i < kOffB2) {
+    const int q = i - kOffW2, n = q / kHidden, k = q % kHidden;
+    w2b[q] = b;
+    w2tb[k * kHidden + n] = b;
+    w2u[umma_k_off(n, k, kHidden)] = b;
+  }
+}
+
 // Adam on the FP32 master parameters, then the BF16 copies the products
 // read (W1, W2 and W2 transposed).  The step counter lives on the device so
 // that a replayed graph keeps counting; adam_step_kernel advances it after
 // every block of this kernel has used it.
 __global__ void adam_kernel(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m1,
                             float* __restrict__ m2, const int* __restrict__ step, AdamHyper h, bf16* __restrict__ w1b,
-                            bf16* __restrict__ w2b, bf16* __restrict__ w2tb) {
+                            bf16* __restrict__ w2b, bf16* __restrict__ w2tb, bf16* __restrict__ w1u,
+                            bf16* __restrict__ w2u) {
   const int t = *step + 1;
   const float c1 = 1.f / (1.f - powf(h.beta1, (float)t));
   const float c2 = 1.f / (1.f - powf(h.beta2, (float)t));
@@ -400,14 +489,7 @@ __global__ void adam_kernel(float* __restrict__ p, const float* __restrict__ g, 
     m2[i] = b;
     const float pi = p[i] - h.lr * (a * c1) / (sqrtf(b * c2) + h.eps);
     p[i] = pi;
-    if (i < kOffB1) {
-      w1b[i] = __float2bfloat16_rn(pi);
-    } else if (i >= kOffW2 && i < kOffB2) {
-      const int q = i - kOffW2, n = q / kHidden, k = q % kHidden;
-      const bf16 v = __float2bfloat16_rn(pi);
-      w2b[q] = v;
-      w2tb[k * kHidden + n] = v;
-    }
+    store_bf16_copies(i, pi, w1b, w2b, w2tb, w1u, w2u);
   }
 }
 
@@ -415,17 +497,9 @@ __global__ void adam_step_kernel(int* step) { *step += 1; }
 
 // BF16 copies of freshly written FP32 parameters.
 __global__ void cast_params_kernel(const float* __restrict__ p, bf16* __restrict__ w1b, bf16* __restrict__ w2b,
-                                   bf16* __restrict__ w2tb) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kParams; i += gridDim.x * blockDim.x) {
-    if (i < kOffB1) {
-      w1b[i] = __float2bfloat16_rn(p[i]);
-    } else if (i >= kOffW2 && i < kOffB2) {
-      const int q = i - kOffW2, n = q / kHidden, k = q % kHidden;
-      const bf16 v = __float2bfloat16_rn(p[i]);
-      w2b[q] = v;
-      w2tb[k * kHidden + n] = v;
-    }
-  }
+                                   bf16* __restrict__ w2tb, bf16* __restrict__ w1u, bf16* __restrict__ w2u) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kParams; i += gridDim.x * blockDim.x)
+    store_bf16_copies(i, p[i], w1b, w2b, w2tb, w1u, w2u);
 }
 
 // Rows idx[0..B) of X (rows 0..B when idx is null) into Xs.
@@ -450,9 +524,9 @@ using namespace mlp;
 int mlp_forward(ggb_mlp* m, const bf16* X, int rows, float* y, cudaStream_t st, bool keep_z) {
   if (rows % 16 || rows > m->max_rows) return core_fail(GGB_EINVAL, "mlp rows %d (max %d, multiple of 16)", rows, m->max_rows);
   if (!keep_z) {
-    // inference: one fused launch, the activations never leave the SM
-    forward_fused_kernel<<<(rows + kFuseRows - 1) / kFuseRows, kFuseThreads, kFuseSmem, st>>>(X, rows, m->W1b, m->W2b,
-                                                                                            m->p, y);
+    // inference: one fused launch on the tcgen05 tensor cores, the activations never leave the SM
+    forward_tc_kernel<<<(rows + tc::kRows - 1) / tc::kRows, tc::kThreads, tc::kSmem, st>>>(X, rows, m->W1u, m->W2u,
+                                                                                         m->p, y);
     core_add_launches(1);
     MCUDA(cudaGetLastError());
     return GGB_OK;
@@ -498,7 +572,7 @@ int mlp_backward(ggb_mlp* m, const bf16* Xs, const float* t, int B, cudaStream_t
 
 int mlp_adam(ggb_mlp* m, cudaStream_t st) {
   adam_kernel<<<(kParams + 255) / 256, 256, 0, st>>>(m->p, m->g, m->m1, m->m2, m->step, m->hyper, m->W1b, m->W2b,
-                                                     m->W2tb);
+                                                     m->W2tb, m->W1u, m->W2u);
   adam_step_kernel<<<1, 1, 0, st>>>(m->step);
   core_add_launches(2);
   MCUDA(cudaGetLastError());
@@ -511,6 +585,33 @@ int mlp_train_rows(ggb_mlp* m, const bf16* X, const int* idx, const float* t, in
   int rc = mlp_backward(m, m->Xs, t, B, st);
   if (rc) return rc;
   return mlp_adam(m, st);
+}
+
+size_t mlp_state_bytes() { return 3 * (size_t)kParams * sizeof(float) + sizeof(int); }
+
+int mlp_save_state(ggb_mlp* m, void* host) {
+  unsigned char* h = static_cast<unsigned char*>(host);
+  const size_t pb = (size_t)kParams * sizeof(float);
+  MCUDA(cudaDeviceSynchronize());
+  MCUDA(cudaMemcpy(h, m->p, pb, cudaMemcpyDeviceToHost));
+  MCUDA(cudaMemcpy(h + pb, m->m1, pb, cudaMemcpyDeviceToHost));
+  MCUDA(cudaMemcpy(h + 2 * pb, m->m2, pb, cudaMemcpyDeviceToHost));
+  MCUDA(cudaMemcpy(h + 3 * pb, m->step, sizeof(int), cudaMemcpyDeviceToHost));
+  return GGB_OK;
+}
+
+int mlp_load_state(ggb_mlp* m, const void* host) {
+  const unsigned char* h = static_cast<const unsigned char*>(host);
+  const size_t pb = (size_t)kParams * sizeof(float);
+  MCUDA(cudaDeviceSynchronize());
+  MCUDA(cudaMemcpy(m->p, h, pb, cudaMemcpyHostToDevice));
+  MCUDA(cudaMemcpy(m->m1, h + pb, pb, cudaMemcpyHostToDevice));
+  MCUDA(cudaMemcpy(m->m2, h + 2 * pb, pb, cudaMemcpyHostToDevice));
+  MCUDA(cudaMemcpy(m->step, h + 3 * pb, sizeof(int), cudaMemcpyHostToDevice));
+  cast_params_kernel<<<64, 256>>>(m->p, m->W1b, m->W2b, m->W2tb, m->W1u, m->W2u);
+  MCUDA(cudaGetLastError());
+  MCUDA(cudaDeviceSynchronize());
+  return GGB_OK;
 }
 
 }  // namespace ggb
@@ -551,12 +652,13 @@ int create(ggb_mlp* m, int max_rows, unsigned long long seed) {
   using namespace ggb::mlp;
   m->max_rows = max_rows;
   int rc;
-  MCUDA(cudaFuncSetAttribute((const void*)forward_fused_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)kFuseSmem));
+  MCUDA(cudaFuncSetAttribute((const void*)forward_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)tc::kSmem));
   const size_t R = (size_t)max_rows;
   if ((rc = mdev(&m->p, kParams)) || (rc = mdev(&m->g, kParams)) || (rc = mdev(&m->m1, kParams)) ||
       (rc = mdev(&m->m2, kParams)) || (rc = mdev(&m->step, 1)) || (rc = mdev(&m->W1b, (size_t)kOffB1)) ||
       (rc = mdev(&m->W2b, (size_t)kHidden * kHidden)) || (rc = mdev(&m->W2tb, (size_t)kHidden * kHidden)) ||
+      (rc = mdev(&m->W1u, (size_t)kOffB1)) || (rc = mdev(&m->W2u, (size_t)kHidden * kHidden)) ||
       (rc = mdev(&m->H1, R * kHidden)) || (rc = mdev(&m->H2, R * kHidden)) || (rc = mdev(&m->Z2, R * kHidden)) ||
       (rc = mdev(&m->y_train, (size_t)kMaxTrainRows)) || (rc = mdev(&m->dZ2, (size_t)kMaxTrainRows * kHidden)) ||
       (rc = mdev(&m->dZ2t, (size_t)kMaxTrainRows * kHidden)) || (rc = mdev(&m->H1t, (size_t)kMaxTrainRows * kHidden)) ||
@@ -573,7 +675,7 @@ int create(ggb_mlp* m, int max_rows, unsigned long long seed) {
 void destroy(ggb_mlp* m) {
   if (!m) return;
   for (void* q : {(void*)m->p, (void*)m->g, (void*)m->m1, (void*)m->m2, (void*)m->step, (void*)m->W1b, (void*)m->W2b,
-                  (void*)m->W2tb, (void*)m->H1, (void*)m->H2, (void*)m->Z2, (void*)m->y_train, (void*)m->dZ2,
+                  (void*)m->W2tb, (void*)m->W1u, (void*)m->W2u, (void*)m->H1, (void*)m->H2, (void*)m->Z2, (void*)m->y_train, (void*)m->dZ2,
                   (void*)m->dZ2t, (void*)m->H1t, (void*)m->dZ1, (void*)m->dZ1f, (void*)m->dZ1t, (void*)m->Xt,
                   (void*)m->Xs, (void*)m->loss, (void*)m->X, (void*)m->y, (void*)m->t})
     cudaFree(q);
@@ -618,7 +720,7 @@ int ggb_mlp_set_params(ggb_mlp* m, const float* params) {
   MCUDA(cudaMemset(m->m1, 0, kParams * sizeof(float)));
   MCUDA(cudaMemset(m->m2, 0, kParams * sizeof(float)));
   MCUDA(cudaMemset(m->step, 0, sizeof(int)));
-  cast_params_kernel<<<64, 256>>>(m->p, m->W1b, m->W2b, m->W2tb);
+  cast_params_kernel<<<64, 256>>>(m->p, m->W1b, m->W2b, m->W2tb, m->W1u, m->W2u);
   MCUDA(cudaGetLastError());
   MCUDA(cudaDeviceSynchronize());
   return GGB_OK;
@@ -646,6 +748,33 @@ int ggb_mlp_forward_host(ggb_mlp* m, const float* x, int rows, float* y) {
   rc = ggb::mlp_forward(m, m->X, rows, m->y, nullptr, false);
   if (rc) return rc;
   MCUDA(cudaMemcpy(y, m->y, (size_t)rows * sizeof(float), cudaMemcpyDeviceToHost));
+  return GGB_OK;
+}
+
+int ggb_mlp_time_forward(ggb_mlp* m, const float* x, int rows, int reps, double* ms) {
+  if (!m || !x || !ms) return core_fail(GGB_EINVAL, "null pointer");
+  if (rows <= 0 || rows % 16 || rows > m->max_rows || reps <= 0)
+    return core_fail(GGB_EINVAL, "rows must be a multiple of 16 up to max_rows, reps positive");
+  int rc = upload_x(m, x, rows);
+  if (rc) return rc;
+  cudaStream_t st;
+  MCUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  rc = ggb::mlp_forward(m, m->X, rows, m->y, st, false);   // warm-up
+  cudaEventRecord(e0, st);
+  for (int i = 0; i < reps && rc == GGB_OK; ++i) rc = ggb::mlp_forward(m, m->X, rows, m->y, st, false);
+  cudaEventRecord(e1, st);
+  const cudaError_t e = cudaEventSynchronize(e1);
+  float t = 0.f;
+  if (rc == GGB_OK && e == cudaSuccess) cudaEventElapsedTime(&t, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaStreamDestroy(st);
+  if (rc) return rc;
+  if (e != cudaSuccess) return core_fail(GGB_ECUDA, "forward timing: %s", cudaGetErrorString(e));
+  *ms = (double)t / reps;
   return GGB_OK;
 }
 

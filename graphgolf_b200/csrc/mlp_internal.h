@@ -39,6 +39,10 @@ struct ggb_mlp {
   __nv_bfloat16* W1b = nullptr;    // [256][32]
   __nv_bfloat16* W2b = nullptr;    // [256][256]
   __nv_bfloat16* W2tb = nullptr;   // W2 transposed
+  // W1 and W2 in the tensor cores' shared-memory operand layout (K-major,
+  // no swizzle: 8-row x 16-byte core matrices), staged by one bulk copy each
+  __nv_bfloat16* W1u = nullptr;    // [256][32] tiled
+  __nv_bfloat16* W2u = nullptr;    // [256][256] tiled
   // activations and workspaces
   __nv_bfloat16* H1 = nullptr;     // [max_rows][256]
   float* H2 = nullptr;             // [max_rows][256]
@@ -70,5 +74,11 @@ int mlp_backward(ggb_mlp* m, const __nv_bfloat16* Xs, const float* t, int B, cud
 int mlp_adam(ggb_mlp* m, cudaStream_t st);
 // Gathers rows idx[0..B) of X, then backward + Adam on them with targets t.
 int mlp_train_rows(ggb_mlp* m, const __nv_bfloat16* X, const int* idx, const float* t, int B, cudaStream_t st);
+// The training state (FP32 parameters, both Adam moments, the Adam step) as
+// host bytes: its size, a copy out and a copy in (which also refreshes every
+// BF16 copy of the weights).  Synchronous.
+size_t mlp_state_bytes();
+int mlp_save_state(ggb_mlp* m, void* host);
+int mlp_load_state(ggb_mlp* m, const void* host);
 
 }  // namespace ggb

@@ -1409,6 +1409,75 @@ int create(ggb_sa* a, int nodes, int degree, int groups, const int* edges, int K
   return GGB_OK;
 }
 
+// ---- checkpoints -------------------------------------------------------------
+// Layout: header, the device State (pointer fields replaced on restore), the
+// current and the best edge lists, and with a filter the network's training
+// state.  Only the library that wrote a checkpoint reads it (state_bytes and
+// the version are checked).
+constexpr unsigned kCkptMagic = 0x31434747u;   // "GGC1"
+constexpr unsigned kCkptVersion = 1u;
+struct CkptHeader {
+  unsigned magic, version, state_bytes, mlp_bytes;
+  int N, d, groups, lines, K, G, compose_max, C, pred_max, learned;
+  int level_cap;   // the base's kept levels (from the first graph's diameter)
+  int delta;       // candidates evaluated against the base (1) or in full (0)
+};
+
+bool same_config(const CkptHeader& x, const CkptHeader& y) {
+  return x.mlp_bytes == y.mlp_bytes && x.N == y.N && x.d == y.d && x.groups == y.groups && x.lines == y.lines &&
+         x.K == y.K && x.G == y.G && x.compose_max == y.compose_max && x.C == y.C && x.pred_max == y.pred_max &&
+         x.learned == y.learned;
+}
+
+// Re-sizes the base to keep levels 0..cap and rebuilds it from the current
+// graph.  A resumed run keeps the level cap of the run it continues: the cap
+// decides which candidates the delta path serves, hence the counters and,
+// with a filter, the training labels.
+int reset_level_cap(ggb_sa* a, int cap) {
+  SCUDA(cudaStreamSynchronize(a->st));
+  drop_graph(a);
+  const int T = a->base_T;
+  for (void** q : {(void**)&a->d_levels, (void**)&a->d_lcounts, (void**)&a->d_winlev, (void**)&a->d_pcounts,
+                   (void**)&a->d_pwinlev, (void**)&a->d_bctrl, (void**)&a->d_bscratch, (void**)&a->d_bres,
+                   (void**)&a->d_dsum, (void**)&a->d_dlev, (void**)&a->d_dout, (void**)&a->d_dpool,
+                   (void**)&a->d_dused, (void**)&a->d_epsum, (void**)&a->d_epecc, (void**)&a->d_eprows,
+                   (void**)&a->d_ephead, (void**)&a->d_epnext, (void**)&a->d_epmisc, (void**)&a->d_epctrl}) {
+    cudaFree(*q);
+    *q = nullptr;
+  }
+  a->level_cap = cap;
+  int rc = alloc_base(a);
+  if (rc) return rc;
+  set_base_team(a, T);
+  return evaluate_current(a);
+}
+
+size_t ckpt_bytes(const ggb_sa* a) {
+  return sizeof(CkptHeader) + sizeof(State) + (size_t)4 * a->lines * sizeof(int) +
+         (a->learned ? ggb::mlp_state_bytes() : 0);
+}
+
+CkptHeader ckpt_header(const ggb_sa* a) {
+  CkptHeader h{};
+  h.magic = kCkptMagic;
+  h.version = kCkptVersion;
+  h.state_bytes = (unsigned)sizeof(State);
+  h.mlp_bytes = a->learned ? (unsigned)ggb::mlp_state_bytes() : 0u;
+  h.N = a->N;
+  h.d = a->d;
+  h.groups = a->groups;
+  h.lines = a->lines;
+  h.K = a->K;
+  h.G = a->G;
+  h.compose_max = a->compose_max;
+  h.C = a->C;
+  h.pred_max = a->pred_max;
+  h.learned = a->learned ? 1 : 0;
+  h.level_cap = a->has_base ? a->level_cap : 0;
+  h.delta = a->delta ? 1 : 0;
+  return h;
+}
+
 }  // namespace
 
 extern "C" {
@@ -1667,6 +1736,103 @@ int ggb_sa_profile(ggb_sa* a, unsigned* stats) {
   rc = check_sticky(a);
   if (rc) return rc;
   SCUDA(cudaMemcpy(stats, a->d_stats, (size_t)a->N * ggb::kStatLevels * sizeof(unsigned), cudaMemcpyDeviceToHost));
+  return GGB_OK;
+}
+
+long long ggb_sa_checkpoint_bytes(const ggb_sa* a) { return a ? (long long)ckpt_bytes(a) : -1; }
+
+int ggb_sa_checkpoint_info(const void* buf, long long bytes, int* nodes, int* degree, int* groups, int* lines) {
+  if (!buf || !nodes || !degree || !groups || !lines) return core_fail(GGB_EINVAL, "null pointer");
+  CkptHeader h;
+  if (bytes < (long long)sizeof h) return core_fail(GGB_EINVAL, "checkpoint too short");
+  std::memcpy(&h, buf, sizeof h);
+  if (h.magic != kCkptMagic || h.version != kCkptVersion || h.state_bytes != (unsigned)sizeof(State))
+    return core_fail(GGB_EINVAL, "not a checkpoint of this library version");
+  *nodes = h.N;
+  *degree = h.d;
+  *groups = h.groups;
+  *lines = h.lines;
+  return GGB_OK;
+}
+
+int ggb_sa_checkpoint_edges(const void* buf, long long bytes, int best, int* edges) {
+  int n = 0, d = 0, g = 0, lines = 0;
+  int rc = ggb_sa_checkpoint_info(buf, bytes, &n, &d, &g, &lines);
+  if (rc) return rc;
+  if (!edges) return core_fail(GGB_EINVAL, "null pointer");
+  const size_t eb = (size_t)2 * lines * sizeof(int);
+  const size_t off = sizeof(CkptHeader) + sizeof(State) + (best ? eb : 0);
+  if (bytes < (long long)(off + eb)) return core_fail(GGB_EINVAL, "checkpoint too short");
+  std::memcpy(edges, static_cast<const unsigned char*>(buf) + off, eb);
+  return GGB_OK;
+}
+
+int ggb_sa_save(ggb_sa* a, void* buf, long long bytes) {
+  if (!a || !buf) return core_fail(GGB_EINVAL, "null pointer");
+  if (bytes < (long long)ckpt_bytes(a)) return core_fail(GGB_EINVAL, "checkpoint buffer of %lld bytes, %zu needed", bytes, ckpt_bytes(a));
+  SCUDA(cudaSetDevice(a->device));
+  int rc = pull_state(a);
+  if (rc) return rc;
+  unsigned char* p = static_cast<unsigned char*>(buf);
+  const CkptHeader h = ckpt_header(a);
+  std::memcpy(p, &h, sizeof h);
+  p += sizeof h;
+  std::memcpy(p, &a->h, sizeof(State));
+  p += sizeof(State);
+  const size_t eb = (size_t)2 * a->lines * sizeof(int);
+  SCUDA(cudaMemcpy(p, a->d_edges, eb, cudaMemcpyDeviceToHost));
+  p += eb;
+  SCUDA(cudaMemcpy(p, a->d_best_edges, eb, cudaMemcpyDeviceToHost));
+  p += eb;
+  if (a->learned) return ggb::mlp_save_state(a->mlp, p);
+  return GGB_OK;
+}
+
+int ggb_sa_restore(ggb_sa* a, const void* buf, long long bytes) {
+  if (!a || !buf) return core_fail(GGB_EINVAL, "null pointer");
+  if (bytes < (long long)sizeof(CkptHeader)) return core_fail(GGB_EINVAL, "checkpoint too short");
+  const unsigned char* p = static_cast<const unsigned char*>(buf);
+  CkptHeader h;
+  std::memcpy(&h, p, sizeof h);
+  const CkptHeader want = ckpt_header(a);
+  if (h.magic != kCkptMagic || h.version != kCkptVersion || h.state_bytes != want.state_bytes)
+    return core_fail(GGB_EINVAL, "not a checkpoint of this library version");
+  if (!same_config(h, want) || (h.level_cap > 0) != (want.level_cap > 0))
+    return core_fail(GGB_EINVAL, "the checkpoint was written by an annealer of another configuration "
+                                 "(nodes, degree, groups, candidates, proposals, composites)");
+  if (h.delta != want.delta)
+    return core_fail(GGB_EINVAL, "the resumed annealer evaluates candidates %s, the saved run did %s",
+                     want.delta ? "against the base" : "in full", h.delta ? "against the base" : "in full");
+  if (bytes < (long long)ckpt_bytes(a)) return core_fail(GGB_EINVAL, "checkpoint too short");
+  p += sizeof h;
+  State s;
+  std::memcpy(&s, p, sizeof s);
+  p += sizeof s;
+  const size_t eb = (size_t)2 * a->lines * sizeof(int);
+  SCUDA(cudaSetDevice(a->device));
+  SCUDA(cudaStreamSynchronize(a->st));
+  // the annealer must hold the checkpoint's current graph, line for line: its
+  // adjacency and, with a base, its kept levels were built from it
+  std::vector<int> cur((size_t)2 * a->lines);
+  SCUDA(cudaMemcpy(cur.data(), a->d_edges, eb, cudaMemcpyDeviceToHost));
+  if (std::memcmp(cur.data(), p, eb) != 0)
+    return core_fail(GGB_EINVAL, "create the annealer from the checkpoint's current edges before restoring");
+  p += eb;
+  int rc;
+  if (a->has_base && h.level_cap != a->level_cap && (rc = reset_level_cap(a, h.level_cap))) return rc;
+  rc = pull_state(a);
+  if (rc) return rc;
+  if (s.cur_diam != a->h.cur_diam || s.cur_total != a->h.cur_total)
+    return core_fail(GGB_EINVAL, "the checkpoint's current values differ from the evaluation of its edges");
+  s.edges = a->h.edges;
+  s.adj = a->h.adj;
+  s.best_edges = a->h.best_edges;
+  a->h = s;
+  rc = push_state(a);
+  if (rc) return rc;
+  SCUDA(cudaMemcpy(a->d_best_edges, p, eb, cudaMemcpyHostToDevice));
+  p += eb;
+  if (a->learned) return ggb::mlp_load_state(a->mlp, p);
   return GGB_OK;
 }
 

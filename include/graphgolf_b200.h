@@ -140,6 +140,12 @@ int ggb_kernel_times(double *ms_ball, double *ms_persistent);
  * in the reference; a measurement utility for the roofline. */
 int ggb_probe_l2_gather(int N, int d, int window_bits, int iters, double *gbs);
 
+/* The L2 streaming ceiling: GB/s at which an L2-resident buffer of `mib` MiB
+ * (1..96) reaches the SMs' shared memory through bulk copies, one CTA per SM
+ * with about 192 KB in flight, averaged over `iters` launches.  No
+ * counterpart in the reference; a measurement utility for the roofline. */
+int ggb_probe_l2_stream(int mib, int iters, double *gbs);
+
 /* ---- host-buffer entry points (copy in, evaluate, copy out) ------------ */
 
 /* General graph: replaces evaluation() of general/evaluation.c:375-391 with
@@ -316,6 +322,10 @@ int ggb_mlp_set_adam(ggb_mlp *m, float lr, float beta1, float beta2, float eps);
 /* y[r] for rows x 32 FP32 features (rounded to BF16 on the way in);
  * rows % 16 == 0, rows <= max_rows. */
 int ggb_mlp_forward_host(ggb_mlp *m, const float *x, int rows, float *y);
+/* Uploads x (as ggb_mlp_forward_host does), then times `reps` back-to-back
+ * launches of the inference forward on the device-resident rows with CUDA
+ * events on one stream; *ms = the mean time of one forward pass. */
+int ggb_mlp_time_forward(ggb_mlp *m, const float *x, int rows, int reps, double *ms);
 /* Loss and gradients (packed like the parameters) of the mean squared error
  * of rows samples against targets t; rows % 16 == 0, rows <= 256. */
 int ggb_mlp_grads_host(ggb_mlp *m, const float *x, const float *t, int rows, float *loss, float *grads);
@@ -410,6 +420,24 @@ int ggb_sa_check_delta(ggb_sa *a, int *compared, int *mismatches, int *unevaluat
 /* Per-vertex level statistics of the current graph, [nodes][32]: entry
  * [v][k] = vertices not within distance k of v. */
 int ggb_sa_profile(ggb_sa *a, unsigned *stats);
+
+/* Checkpoint and resume of an annealing run.  The reference resumes a run
+ * from the graph it wrote with -o, re-read with -M (general/main.c:444-451,
+ * 367-373), with a fresh temperature and random stream; a checkpoint here
+ * also keeps the step count (which keys the device's counter-based random
+ * stream), the temperature and schedule, the counters, the best graph and,
+ * with a filter, the network's parameters and Adam state, so that a resumed
+ * run continues the interrupted one step for step.  To resume: read the
+ * current edges out of the checkpoint (ggb_sa_checkpoint_edges, best = 0),
+ * create an annealer from them with the same arguments (and the same
+ * ggb_sa_set_predicted / ggb_sa_set_grid calls), then ggb_sa_restore.  Only
+ * the library version that wrote a checkpoint reads it. */
+long long ggb_sa_checkpoint_bytes(const ggb_sa *a);
+int ggb_sa_save(ggb_sa *a, void *buf, long long bytes);
+int ggb_sa_restore(ggb_sa *a, const void *buf, long long bytes);
+int ggb_sa_checkpoint_info(const void *buf, long long bytes, int *nodes, int *degree, int *groups, int *lines);
+/* Current (best = 0) or best (best = 1) edges of a checkpoint, [lines][2]. */
+int ggb_sa_checkpoint_edges(const void *buf, long long bytes, int best, int *edges);
 
 #ifdef __cplusplus
 }

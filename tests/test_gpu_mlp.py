@@ -83,3 +83,41 @@ def test_training_fits(net):
     first = net.grads(x, t)[0]
     last = net.train(x, t, 400)
     assert last < 0.1 * first
+
+
+@pytest.mark.parametrize("rows", [208, 4000])
+def test_forward_partial_tiles(net, rows):
+    """Row counts that leave the last 128-row tile of the inference forward
+    part-filled: every row is written and equals the oracle."""
+    rng = np.random.default_rng(rows)
+    p = mo.init(17)
+    net.params = p
+    x = rng.uniform(-1, 1, (rows, 32)).astype(np.float32)
+    y = net.forward(x)
+    y_ref, _ = mo.forward(p, x)
+    assert np.isfinite(y).all()
+    assert np.abs(y - y_ref).max() <= 0.02 * (np.abs(y_ref).max() + 1e-6)
+
+
+def test_forward_after_adam(net):
+    """Adam refreshes every BF16 copy the forwards read (row-major and the
+    tensor cores' operand layout): after training, the forward equals the
+    oracle's forward with the trained parameters."""
+    rng = np.random.default_rng(31)
+    net.params = mo.init(3, scale=0.5)
+    net.set_adam(lr=3e-3)
+    x = rng.uniform(-1, 1, (128, 32)).astype(np.float32)
+    t = rng.uniform(-1, 1, 128).astype(np.float32)
+    net.train(x, t, 20)
+    p = net.params
+    xs = rng.uniform(-1, 1, (512, 32)).astype(np.float32)
+    y = net.forward(xs)
+    y_ref, _ = mo.forward(p, xs)
+    assert np.abs(y - y_ref).max() <= 0.02 * (np.abs(y_ref).max() + 1e-6)
+
+
+def test_forward_timing(net):
+    net.params = mo.init(5)
+    x = np.random.default_rng(2).uniform(-1, 1, (4096, 32)).astype(np.float32)
+    ms = net.time_forward(x, 20)
+    assert 0.0 < ms < 5.0

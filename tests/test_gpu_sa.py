@@ -299,3 +299,50 @@ def test_orbit_and_grid_inputs_rejected(gpu):
     with gg.Annealer(gr, candidates=4) as an:
         with pytest.raises(gg.EvaluationError):
             an.grid(20, 1)   # the current graph already has longer edges
+
+
+@pytest.mark.parametrize("K,G,comp,metropolis", [(1, 1, 0, True), (16, 16, 8, False), (32, 256, 16, True)])
+def test_checkpoint_resume_identical(gpu, K, G, comp, metropolis):
+    """A run saved after 15 steps and resumed in a fresh annealer continues
+    step for step: the same counters, temperature, current and best graphs as
+    the run that was never interrupted (the step count keys the device's
+    random stream; with a filter, the network's parameters and Adam state
+    travel in the checkpoint too)."""
+    g = graphs.random_regular(1024, 8, 5)
+
+    def make(graph):
+        an = gg.Annealer(graph, candidates=K, proposals=G, compose=comp, seed=9)
+        if metropolis:
+            an.schedule(temp=40.0, cooling=0.97, hill_climbing=False)
+        return an
+
+    with make(g) as a:
+        a.run(15)
+        ck = a.save()
+        full = a.run(15)
+        cur, best = a.edges(), a.edges(best=True)
+    g2 = gg.checkpoint_graph(ck)
+    assert g2.nodes == g.nodes and g2.degree == g.degree
+    with make(g2) as b:
+        b.restore(ck)
+        resumed = b.run(15)
+        assert resumed == full
+        assert np.array_equal(b.edges(), cur) and np.array_equal(b.edges(best=True), best)
+        _check(b, g, resumed)
+
+
+def test_checkpoint_rejects_other_annealers(gpu):
+    g = graphs.random_regular(512, 6, 2)
+    with gg.Annealer(g, candidates=8, seed=1) as a:
+        assert a.run(20).accepts > 0
+        ck = a.save()
+    with gg.Annealer(g, candidates=8, seed=1) as b:      # not the checkpoint's current graph
+        with pytest.raises(gg.EvaluationError):
+            b.restore(ck)
+    with gg.Annealer(gg.checkpoint_graph(ck), candidates=16, seed=1) as c:   # another configuration
+        with pytest.raises(gg.EvaluationError):
+            c.restore(ck)
+    bad = bytearray(ck)
+    bad[0] ^= 0xFF
+    with pytest.raises(gg.EvaluationError):
+        gg.checkpoint_graph(bytes(bad))

@@ -73,3 +73,18 @@ def test_finish_conventions():
     out = _native.ggb_result()
     assert lib.ggb_finish_grid(10, ctypes.byref(p), ctypes.byref(out)) == 0
     assert (out.connected, out.diameter) == (0, 11)
+
+
+def test_checkpoint_parsing_rejects_foreign_bytes():
+    """Reading a checkpoint's header is host-only: bytes that are not a
+    checkpoint of this library are rejected, never interpreted."""
+    import numpy as np
+    lib = _native.load("core")
+    n, d, g, lines = (ctypes.c_int() for _ in range(4))
+    for blob in (b"", b"\x00" * 16, bytes(range(256)) * 8):
+        assert lib.ggb_sa_checkpoint_info(blob, len(blob), ctypes.byref(n), ctypes.byref(d), ctypes.byref(g),
+                                          ctypes.byref(lines)) != 0
+        e = np.empty(16, dtype=np.int32)
+        assert lib.ggb_sa_checkpoint_edges(blob, len(blob), 0, e.ctypes.data) != 0
+    with pytest.raises(gg.EvaluationError):
+        gg.checkpoint_graph(b"\x31\x47\x47\x43" + b"\x00" * 60)
