@@ -741,6 +741,7 @@ struct ggb_sa {
   bool learned = false;
   bool delta = false;             // candidates evaluated against the base, not in full
   bool has_base = false;          // the base is kept (delta evaluation, the filter's features)
+  bool broken = false;            // a restore failed while re-sizing the base: only destroy is allowed
   State h{};                      // host mirror of the device state
   State* d_state = nullptr;
   int* d_edges = nullptr;
@@ -1446,10 +1447,17 @@ int reset_level_cap(ggb_sa* a, int cap) {
     *q = nullptr;
   }
   a->level_cap = cap;
+  a->broken = true;   // until the base is whole again
   int rc = alloc_base(a);
   if (rc) return rc;
   set_base_team(a, T);
-  return evaluate_current(a);
+  rc = evaluate_current(a);
+  if (rc == GGB_OK) a->broken = false;
+  return rc;
+}
+
+int refuse_broken(const ggb_sa* a) {
+  return core_fail(GGB_EPERM, "a restore of this annealer failed while re-sizing its base; destroy it");
 }
 
 size_t ckpt_bytes(const ggb_sa* a) {
@@ -1559,6 +1567,7 @@ void ggb_sa_destroy(ggb_sa* a) { destroy(a); }
 
 int ggb_sa_set_schedule(ggb_sa* a, double temp, double cooling_rate, int hill_climbing) {
   if (!a) return core_fail(GGB_EINVAL, "null annealer");
+  if (a->broken) return refuse_broken(a);
   if (!(temp >= 0.0) || !(cooling_rate > 0.0)) return core_fail(GGB_EINVAL, "temp >= 0 and cooling_rate > 0");
   if (!hill_climbing && !(temp > 0.0)) return core_fail(GGB_EINVAL, "annealing needs temp > 0");
   SCUDA(cudaSetDevice(a->device));
@@ -1615,6 +1624,7 @@ int ggb_sa_set_target(ggb_sa* a, int diameter, long long total) {
 
 int ggb_sa_autotune(ggb_sa* a, int iters, int* window_bits, int* team_ctas, double* best_ms) {
   if (!a) return core_fail(GGB_EINVAL, "null annealer");
+  if (a->broken) return refuse_broken(a);
   SCUDA(cudaSetDevice(a->device));
   drop_graph(a);
   ggb_batch* b = a->cand ? a->cand : a->comp;
@@ -1629,6 +1639,7 @@ int ggb_sa_autotune(ggb_sa* a, int iters, int* window_bits, int* team_ctas, doub
 
 int ggb_sa_run(ggb_sa* a, long long steps, ggb_sa_stats* stats) {
   if (!a || steps < 0) return core_fail(GGB_EINVAL, "null annealer or negative steps");
+  if (a->broken) return refuse_broken(a);
   SCUDA(cudaSetDevice(a->device));
   int rc = capture_step(a);
   if (rc) return rc;
@@ -1687,6 +1698,7 @@ int ggb_sa_last_step(ggb_sa* a, float* predicted, float* label) {
 int ggb_sa_check_delta(ggb_sa* a, int* compared, int* mismatches, int* unevaluated, int* dense_windows) {
   using namespace ggb::sa;
   if (!a || !compared || !mismatches || !unevaluated) return core_fail(GGB_EINVAL, "null pointer");
+  if (a->broken) return refuse_broken(a);
   if (!a->has_base) return core_fail(GGB_EPERM, "the annealer keeps no base for the delta evaluation");
   SCUDA(cudaSetDevice(a->device));
   int rc = pull_state(a);
@@ -1728,6 +1740,7 @@ int ggb_sa_check_delta(ggb_sa* a, int* compared, int* mismatches, int* unevaluat
 
 int ggb_sa_profile(ggb_sa* a, unsigned* stats) {
   if (!a || !stats) return core_fail(GGB_EINVAL, "null pointer");
+  if (a->broken) return refuse_broken(a);
   SCUDA(cudaSetDevice(a->device));
   // the statistics the features read: from the base build when it makes them
   int rc = a->has_base ? enqueue_base(a, nullptr, a->st) : enqueue_profile(a, nullptr, a->st);
@@ -1769,6 +1782,7 @@ int ggb_sa_checkpoint_edges(const void* buf, long long bytes, int best, int* edg
 
 int ggb_sa_save(ggb_sa* a, void* buf, long long bytes) {
   if (!a || !buf) return core_fail(GGB_EINVAL, "null pointer");
+  if (a->broken) return refuse_broken(a);
   if (bytes < (long long)ckpt_bytes(a)) return core_fail(GGB_EINVAL, "checkpoint buffer of %lld bytes, %zu needed", bytes, ckpt_bytes(a));
   SCUDA(cudaSetDevice(a->device));
   int rc = pull_state(a);
@@ -1790,6 +1804,7 @@ int ggb_sa_save(ggb_sa* a, void* buf, long long bytes) {
 
 int ggb_sa_restore(ggb_sa* a, const void* buf, long long bytes) {
   if (!a || !buf) return core_fail(GGB_EINVAL, "null pointer");
+  if (a->broken) return refuse_broken(a);
   if (bytes < (long long)sizeof(CkptHeader)) return core_fail(GGB_EINVAL, "checkpoint too short");
   const unsigned char* p = static_cast<const unsigned char*>(buf);
   CkptHeader h;

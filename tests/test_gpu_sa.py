@@ -346,3 +346,26 @@ def test_checkpoint_rejects_other_annealers(gpu):
     bad[0] ^= 0xFF
     with pytest.raises(gg.EvaluationError):
         gg.checkpoint_graph(bytes(bad))
+
+
+def test_checkpoint_with_another_level_cap(gpu):
+    """A checkpoint whose base kept more levels than the resuming annealer's
+    first graph needs (its run started from a graph of larger diameter): the
+    restore re-sizes the base to the saved cap and rebuilds it, and the
+    resumed run's states are exact.  The cap is the header's 15th 32-bit
+    field; raising it by one stands in for a run whose diameter has dropped."""
+    import struct
+    g = graphs.random_regular(1024, 8, 6)
+    with gg.Annealer(g, candidates=16, compose=8, seed=4) as a:
+        a.run(10)
+        ck = bytearray(a.save())
+    cap = struct.unpack_from("<i", ck, 56)[0]
+    assert cap >= 2
+    struct.pack_into("<i", ck, 56, cap + 1)
+    with gg.Annealer(gg.checkpoint_graph(bytes(ck)), candidates=16, compose=8, seed=4) as b:
+        b.restore(bytes(ck))
+        st = b.run(10)
+        assert st.step == 20
+        _check(b, g, st)
+        compared, bad, _ = b.check_delta()
+        assert compared > 0 and bad == 0
