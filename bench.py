@@ -748,6 +748,7 @@ def _race(g, plain_steps: int, schedule, rows) -> dict:
         if G > K:
             a.predicted(0, 1)
         a.target(st.best_diam, st.best_total)
+        plan = a.base_plan()
         s = a.run(0)
         t0 = time.perf_counter()
         while not s.done and time.perf_counter() - t0 < 90:
@@ -759,7 +760,8 @@ def _race(g, plain_steps: int, schedule, rows) -> dict:
         out[name] = {"wall_s": el, "reached": bool(s.done), "steps": s.step, "accepts": s.accepts,
                      "moved_swaps": s.moved_swaps, "evals": s.evals, "final_aspl": s.cur_aspl,
                      "final_checked": (r.diameter, r.total) == (s.cur_diam, s.cur_total),
-                     "candidates": K, "proposals": G, "speedup_vs_plain": t_plain / el if s.done else None}
+                     "candidates": K, "proposals": G, "speedup_vs_plain": t_plain / el if s.done else None,
+                     "base_plan": {"team_ctas": plan[0], "teams": plan[1]}}
     return out
 
 

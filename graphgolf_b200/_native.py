@@ -140,6 +140,7 @@ CORE_SIGNATURES = {
     "ggb_sa_run": (_I, [_P, _LL, C.POINTER(ggb_sa_stats)]),
     "ggb_sa_edges": (_I, [_P, _I, _P]),
     "ggb_sa_profile": (_I, [_P, _P]),
+    "ggb_sa_base_plan": (_I, [_P, _IP, _IP]),
     "ggb_sa_checkpoint_bytes": (_LL, [_P]),
     "ggb_sa_save": (_I, [_P, _P, _LL]),
     "ggb_sa_restore": (_I, [_P, _P, _LL]),

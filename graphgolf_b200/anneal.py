@@ -129,6 +129,12 @@ class Annealer:
         _raise(self._lib.ggb_sa_check_delta(self._h, C.byref(c), C.byref(m), C.byref(u), C.byref(dn)))
         return (c.value, m.value, u.value, dn.value) if with_dense else (c.value, m.value, u.value)
 
+    def base_plan(self) -> tuple[int, int]:
+        """(CTAs per team, teams) of the kept base's build, (0, 0) without one."""
+        t, n = C.c_int(), C.c_int()
+        _raise(self._lib.ggb_sa_base_plan(self._h, C.byref(t), C.byref(n)))
+        return t.value, n.value
+
     def save(self) -> bytes:
         """A checkpoint of the run: graph, best graph, step, schedule,
         counters and (with a filter) the network's training state."""

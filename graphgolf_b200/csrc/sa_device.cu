@@ -1164,27 +1164,38 @@ void set_base_team(ggb_sa* a, int T) {
 // whole GPU (two launches each after one warm-up) and keeps the fastest.  The
 // result never depends on the choice.
 int tune_base(ggb_sa* a) {
+  // Each team size is timed in three rounds of one warm-up and two timed
+  // builds, the rounds interleaved so that a clock ramp or a noisy moment
+  // does not decide the choice; the least time of a size's rounds counts.
   cudaEvent_t e0, e1;
   SCUDA(cudaEventCreate(&e0));
   SCUDA(cudaEventCreate(&e1));
-  float best = 1e30f;
-  int bestT = 4;
-  for (int T : {1, 2, 4, 8, 16, std::max(1, a->sms / a->nbw)}) {
-    if (T > a->sms) continue;
-    set_base_team(a, T);
-    int rc = enqueue_base(a, nullptr, a->st);
-    if (rc) return rc;
-    SCUDA(cudaEventRecord(e0, a->st));
-    for (int i = 0; i < 2 && !rc; ++i) rc = enqueue_base(a, nullptr, a->st);
-    if (rc) return rc;
-    SCUDA(cudaEventRecord(e1, a->st));
-    SCUDA(cudaEventSynchronize(e1));
-    float ms = 0.f;
-    SCUDA(cudaEventElapsedTime(&ms, e0, e1));
-    if (ms < best) { best = ms; bestT = T; }
+  const int sizes[] = {1, 2, 4, 8, 16, std::max(1, a->sms / a->nbw)};
+  float best_ms[6];
+  for (float& b : best_ms) b = 1e30f;
+  for (int round = 0; round < 3; ++round) {
+    for (int i = 0; i < 6; ++i) {
+      const int T = sizes[i];
+      if (T > a->sms) continue;
+      set_base_team(a, T);
+      int rc = enqueue_base(a, nullptr, a->st);
+      if (rc) return rc;
+      SCUDA(cudaEventRecord(e0, a->st));
+      for (int k = 0; k < 2 && !rc; ++k) rc = enqueue_base(a, nullptr, a->st);
+      if (rc) return rc;
+      SCUDA(cudaEventRecord(e1, a->st));
+      SCUDA(cudaEventSynchronize(e1));
+      float ms = 0.f;
+      SCUDA(cudaEventElapsedTime(&ms, e0, e1));
+      best_ms[i] = std::min(best_ms[i], ms);
+    }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  int bestT = 4;
+  float best = 1e30f;
+  for (int i = 0; i < 6; ++i)
+    if (sizes[i] <= a->sms && best_ms[i] < best) { best = best_ms[i]; bestT = sizes[i]; }
   set_base_team(a, bestT);
   return check_sticky(a);
 }
@@ -1749,6 +1760,13 @@ int ggb_sa_profile(ggb_sa* a, unsigned* stats) {
   rc = check_sticky(a);
   if (rc) return rc;
   SCUDA(cudaMemcpy(stats, a->d_stats, (size_t)a->N * ggb::kStatLevels * sizeof(unsigned), cudaMemcpyDeviceToHost));
+  return GGB_OK;
+}
+
+int ggb_sa_base_plan(const ggb_sa* a, int* team_ctas, int* teams) {
+  if (!a || !team_ctas || !teams) return core_fail(GGB_EINVAL, "null pointer");
+  *team_ctas = a->has_base ? a->base_T : 0;
+  *teams = a->has_base ? a->base_teams : 0;
   return GGB_OK;
 }
 

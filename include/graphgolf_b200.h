@@ -417,6 +417,9 @@ int ggb_sa_last_step(ggb_sa *a, float *predicted, float *label);
  * sum among those the delta path served; dense_windows (may be NULL)
  * receives how many (candidate, window) tasks fell back to a dense sweep. */
 int ggb_sa_check_delta(ggb_sa *a, int *compared, int *mismatches, int *unevaluated, int *dense_windows);
+/* The kept base's build plan, timed at creation: CTAs per team and teams
+ * (0, 0 without a base). */
+int ggb_sa_base_plan(const ggb_sa *a, int *team_ctas, int *teams);
 /* Per-vertex level statistics of the current graph, [nodes][32]: entry
  * [v][k] = vertices not within distance k of v. */
 int ggb_sa_profile(ggb_sa *a, unsigned *stats);
