@@ -210,20 +210,22 @@ extern "C" int ggb_probe_l2_stream(int mib, int iters, double* gbs) {
   cudaMemset(buf, 0x5a, (size_t)chunks * kStreamChunk);
   cudaMemset(err, 0, sizeof(int));
   constexpr int kPasses = 16;   // 1 GiB a launch at 64 MiB, so the launch gaps stay small
-  probe_stream_kernel<<<sms, 32, smem>>>(buf, chunks, kPasses, err);
-  cudaEvent_t e0, e1;
-  cudaEventCreate(&e0);
-  cudaEventCreate(&e1);
-  cudaEventRecord(e0);
-  for (int it = 0; it < iters; ++it) probe_stream_kernel<<<sms, 32, smem>>>(buf, chunks, kPasses, err);
-  cudaEventRecord(e1);
-  cudaError_t e = cudaEventSynchronize(e1);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  cudaError_t e = cudaEventCreate(&e0);
+  if (e == cudaSuccess) e = cudaEventCreate(&e1);
   float ms = 0.f;
-  if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
   int h_err = 0;
-  if (e == cudaSuccess) e = cudaMemcpy(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost);
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
+  if (e == cudaSuccess) {
+    probe_stream_kernel<<<sms, 32, smem>>>(buf, chunks, kPasses, err);   // warm-up: the buffer into L2
+    e = cudaEventRecord(e0);
+    for (int it = 0; it < iters && e == cudaSuccess; ++it) probe_stream_kernel<<<sms, 32, smem>>>(buf, chunks, kPasses, err);
+    if (e == cudaSuccess) e = cudaEventRecord(e1);
+    if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+    if (e == cudaSuccess) e = cudaMemcpy(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost);
+  }
+  if (e1) cudaEventDestroy(e1);
+  if (e0) cudaEventDestroy(e0);
   cudaFree(buf);
   cudaFree(err);
   if (e != cudaSuccess) {

@@ -757,21 +757,27 @@ int ggb_mlp_time_forward(ggb_mlp* m, const float* x, int rows, int reps, double*
     return core_fail(GGB_EINVAL, "rows must be a multiple of 16 up to max_rows, reps positive");
   int rc = upload_x(m, x, rows);
   if (rc) return rc;
-  cudaStream_t st;
-  MCUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-  cudaEvent_t e0, e1;
-  cudaEventCreate(&e0);
-  cudaEventCreate(&e1);
-  rc = ggb::mlp_forward(m, m->X, rows, m->y, st, false);   // warm-up
-  cudaEventRecord(e0, st);
-  for (int i = 0; i < reps && rc == GGB_OK; ++i) rc = ggb::mlp_forward(m, m->X, rows, m->y, st, false);
-  cudaEventRecord(e1, st);
-  const cudaError_t e = cudaEventSynchronize(e1);
+  cudaStream_t st = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreate(&e0);
+  if (e == cudaSuccess) e = cudaEventCreate(&e1);
   float t = 0.f;
-  if (rc == GGB_OK && e == cudaSuccess) cudaEventElapsedTime(&t, e0, e1);
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
-  cudaStreamDestroy(st);
+  if (e == cudaSuccess) {
+    rc = ggb::mlp_forward(m, m->X, rows, m->y, st, false);   // warm-up
+    if (rc == GGB_OK) e = cudaEventRecord(e0, st);
+    for (int i = 0; i < reps && rc == GGB_OK && e == cudaSuccess; ++i)
+      rc = ggb::mlp_forward(m, m->X, rows, m->y, st, false);
+    if (rc == GGB_OK && e == cudaSuccess) e = cudaEventRecord(e1, st);
+    if (rc == GGB_OK && e == cudaSuccess) e = cudaEventSynchronize(e1);
+    if (rc == GGB_OK && e == cudaSuccess) e = cudaEventElapsedTime(&t, e0, e1);
+  }
+  if (e1) cudaEventDestroy(e1);
+  if (e0) cudaEventDestroy(e0);
+  if (st) {
+    cudaStreamSynchronize(st);
+    cudaStreamDestroy(st);
+  }
   if (rc) return rc;
   if (e != cudaSuccess) return core_fail(GGB_ECUDA, "forward timing: %s", cudaGetErrorString(e));
   *ms = (double)t / reps;
