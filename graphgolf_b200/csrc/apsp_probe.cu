@@ -2,15 +2,15 @@
 //
 // The sweeps' working set (two bitset matrices of a source window) is
 // L2-resident by design, so the roof that bounds them is not the HBM copy
-// bandwidth but the rate at which the SMs can gather random rows of that size
-// from L2.  ggb_probe_l2_gather times exactly that access pattern -- every
-// vertex ORs its own row and the rows of its d random neighbours out of a
-// matrix of the same shape, with the same 32-byte accesses, one launch per
-// sweep, at two CTAs per SM -- on buffers it allocates itself, and reports
-// the sweep's algorithmic bytes per second.  bench.py uses it as the roof of
-// its roofline report.  ggb_probe_l2_stream measures the ceiling above it:
-// the rate at which L2 delivers an L2-resident buffer to the SMs, with bulk
-// copies that keep far more bytes in flight than registers can.
+// bandwidth but the rate at which L2 delivers bytes to the SMs.
+// ggb_probe_l2_stream measures that ceiling: bulk copies of an L2-resident
+// buffer into shared memory, which keep far more bytes in flight than
+// registers can; bench.py reports it as the roofline's peak.
+// ggb_probe_l2_gather times the sweeps' own access pattern -- every vertex
+// ORs its own row and the rows of its d random neighbours out of a matrix of
+// the same shape, with the same 32-byte accesses, one launch per sweep, at
+// two CTAs per SM -- on buffers it allocates itself, and reports the sweep's
+// algorithmic bytes per second, beside the peak.
 #include <cuda_runtime.h>
 
 #include <algorithm>

@@ -131,19 +131,20 @@ int ggb_trace_read(long long *out, int max_pairs);
 int ggb_set_timing(int enable);
 int ggb_kernel_times(double *ms_ball, double *ms_persistent);
 
-/* The roof the dense sweeps run against: random-row OR sweeps (d random
- * neighbours per row, rows of window_bits/8 bytes, N rows) with the sweeps'
- * own access width (32-byte loads for rows of 32 bytes or more), one launch
- * per sweep, on the current device with its own buffers.  *gbs counts the
- * algorithmic bytes of a dense sweep (N*d*4 + N*d*W/8 + 2*N*W/8) per second,
- * the figure bench.py's roofline reports for the evaluator.  No counterpart
+/* The dense sweeps' own access pattern as a probe: random-row OR sweeps (d
+ * random neighbours per row, rows of window_bits/8 bytes, N rows) with the
+ * sweeps' access width (32-byte loads for rows of 32 bytes or more), one
+ * launch per sweep, on the current device with its own buffers.  *gbs counts
+ * the algorithmic bytes of a dense sweep (N*d*4 + N*d*W/8 + 2*N*W/8) per
+ * second; bench.py reports it beside the roofline's peak.  No counterpart
  * in the reference; a measurement utility for the roofline. */
 int ggb_probe_l2_gather(int N, int d, int window_bits, int iters, double *gbs);
 
-/* The L2 streaming ceiling: GB/s at which an L2-resident buffer of `mib` MiB
- * (1..96) reaches the SMs' shared memory through bulk copies, one CTA per SM
- * with about 192 KB in flight, averaged over `iters` launches.  No
- * counterpart in the reference; a measurement utility for the roofline. */
+/* The L2 streaming ceiling, the roofline's peak in bench.py: GB/s at which an
+ * L2-resident buffer of `mib` MiB (1..96) reaches the SMs' shared memory
+ * through bulk copies, one CTA per SM with about 192 KB in flight, averaged
+ * over `iters` launches.  No counterpart in the reference; a measurement
+ * utility for the roofline. */
 int ggb_probe_l2_stream(int mib, int iters, double *gbs);
 
 /* ---- host-buffer entry points (copy in, evaluate, copy out) ------------ */
