@@ -715,7 +715,7 @@ def batch_bench(peak: float, peak_kind: str, lib) -> dict:
     b.close()
     roof = roofline(f"apsp_batch_kernel<{bits // 128}>", alg, kms, l2, peak, peak_kind, None, None,
                     l2_stream=l2_stream_roof(lib))
-    roof["peak_source"] += " (probed at N=16384, d=12: the largest graphs of the batch)"
+    roof["l2_gather_probe_case"] = "N=16384, d=12: the largest graphs of the batch"
     return {"workload": "4096-vertex base + 256 single-swap candidates, d=12, N log-uniform 512..16384",
             "graphs": len(w), "plan": {"window_bits": bits, "team_ctas": team, "autotune_s": tune_s},
             "value": len(w) / (kms / 1e3), "unit": "graphs/s", "ms_per_batch": kms,
