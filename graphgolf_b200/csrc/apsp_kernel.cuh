@@ -905,6 +905,19 @@ __device__ __forceinline__ void sweep_stamped(const uint4* __restrict__ src, uin
   }
 }
 
+// Drops every full 128-byte line of [p, p + cells * 16) from L2 without a
+// write-back (discard.global.L2), the lines split over the threads of CTAs
+// cta .. ncta - 1.  Lines that straddle the range's ends are left alone.
+__device__ __forceinline__ void discard_l2(const void* p, size_t cells, int cta, int ncta) {
+  const unsigned long long b = (unsigned long long)p, e = b + (unsigned long long)cells * 16ull;
+  const unsigned long long first = (b + 127ull) & ~127ull, last = e & ~127ull;
+  if (last <= first) return;
+  const unsigned long long lines = (last - first) >> 7;
+  for (unsigned long long i = (unsigned long long)cta * kThreads + threadIdx.x; i < lines;
+       i += (unsigned long long)ncta * kThreads)
+    asm volatile("discard.global.L2 [%0], 128;" ::"l"(first + (i << 7)) : "memory");
+}
+
 // ---- one graph on a team of CTAs ------------------------------------------------
 // R = uint4 words per row (W = 128*R source bits).  LPR lanes share a row,
 // each lane owning UPL uint4 of it; a warp covers VPW vertices per step.
@@ -1013,6 +1026,12 @@ __device__ __forceinline__ bool eval_windows(const ApspArgs& a, int cta, int nct
         own_count = true;
         cur = a.ball + (size_t)local * N * R;
         nxt = a.buf0;
+        // buf1 holds the previous window's rows, all dead: this window's first
+        // sweep writes buf0 only, and every later reader of buf1 reads rows
+        // written in this window.  Dropping those dirty lines from L2 saves
+        // their write-back to DRAM; the grid barrier that ends the first sweep
+        // orders the drops before the second sweep writes buf1.
+        if (!lev0 && local > 0 && !act) discard_l2(a.buf1, (size_t)N * R, cta, ncta);
       } else {
         // ---- levels 0 and 1 by two-hop seeding into buf0 -----------------------
         unsigned c[4] = {0u, 0u, 0u, 0u};  // S_1 lo, S_1 hi, S_2 lo, S_2 hi
