@@ -88,3 +88,12 @@ def test_checkpoint_parsing_rejects_foreign_bytes():
         assert lib.ggb_sa_checkpoint_edges(blob, len(blob), 0, e.ctypes.data) != 0
     with pytest.raises(gg.EvaluationError):
         gg.checkpoint_graph(b"\x31\x47\x47\x43" + b"\x00" * 60)
+
+
+def test_every_declared_function_has_a_binding():
+    """Every ggb_* function the header declares has a ctypes signature in the
+    package's binding table, so Python callers never fall back to ctypes'
+    default int/pointer guesses."""
+    names = _declared()
+    missing = [n for n in names if n not in _native.CORE_SIGNATURES]
+    assert not missing, missing
